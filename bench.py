@@ -1,0 +1,291 @@
+#!/usr/bin/env python
+"""Benchmark: particle-updates/s of the MPH-WC explicit step, 3-D dam break.
+
+Workload (default): 100x100x200 type-0 fluid block (2.0 M particles, l0 =
+0.005 m, seeded +-0.01 l0 jitter) in the corner of a 300x100x240-cell box closed
+by 3 layers of type-2 wall particles (0.78 M), gravity -9.81 z, rho 1000,
+mu 1e-3, no surface tension, radii 1.7/3.5 l0, c = 20 m/s, dt 2e-5 s.
+Synthetic data from the seeded generator (mphexplicit_b200/scenes.py); the
+reference publishes no input set for it.
+
+A "step" is one explicit step of the whole scene (the reference's loop body).
+value = fluid particles x steps / seconds, summed over ranks (replicas: the
+step does not shard, each rank runs its own scene on its own GPU).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed]
+  python bench.py --impl reference ...   # the reference's own CPU step, all host threads
+
+One JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s, 3D 2M-particle dam break: FP64 plain vs mixed/learned"
+UNIT = "particle-updates/s"
+# algorithmic HBM bytes per particle per launch, 3-D without surface tension:
+# sweep A reads x, v, type (52 B) and writes PressureP (8 B); sweep B reads
+# x, v, type, PressureP (60 B) and writes x, v (48 B)  -> 168 B per update.
+ALGO_BYTES = {"sweep_a": 60.0, "sweep_b": 108.0, "move": 96.0}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` on the bench workload, from the
+    committed ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_%s_dam_break_3d.md" % kernel)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_launch_full_size:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--id=%d" % self.idx, "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_scene(args, rank):
+    from mphexplicit_b200 import scenes
+    if args.scene == "dam":
+        return scenes.dam_break_3d(seed=rank)
+    if args.scene == "dam_small":
+        return scenes.dam_break_3d(fluid=(40, 40, 80), box=(120, 40, 96), seed=rank)
+    raise SystemExit("unknown scene " + args.scene)
+
+
+def workload_name(sc) -> str:
+    m = sc.meta
+    return ("dam_break_3d fluid %dx%dx%d in a %dx%dx%d-cell box, %d wall layers, l0=%g: %d particles (%d fluid)"
+            % (*m["fluid"], *m["box"], m["walls"], m["l0"], sc.n, sc.n_fluid))
+
+
+def cpu_baseline(sc, seconds_budget: float, steps: int):
+    """The reference's own step (oracle/_ref, OpenMP, all host threads) on the
+    same scene; a bounded sample: the steps that fit in the budget."""
+    from oracle import pyoracle as po
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        d, g = os.path.join(td, "b.data"), os.path.join(td, "b.grid")
+        sc.write(d, g)
+        if po.ref_available(sc.dim):
+            r = po.time_reference(d, g, sc.dim, 0, steps, threads, max_seconds=seconds_budget, timeout=1800)
+            kind = "reference"
+        else:
+            os.environ["OMP_NUM_THREADS"] = str(threads)
+            r = po.time_oracle(sc, 0, steps, max_seconds=seconds_budget)
+            kind = "port"
+    val = r["fluid"] * r["steps"] / r["seconds"]
+    return {"value": val, "unit": UNIT, "cores": r["threads"], "kind": kind,
+            "sample": "%d step(s) of the full %d-particle scene (%d fluid), %d rebuild(s), %.1f s wall"
+                      % (r["steps"], r["particles"], r["fluid"], r["rebuilds"], r["seconds"])}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    sc = make_scene(args, 0)
+    steps = max(1, min(args.steps, args.ref_max_steps))
+    base = cpu_baseline(sc, args.ref_seconds, steps)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": workload_name(sc), "mode": "reference CPU (OpenMP)"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--scene", default="dam", choices=["dam", "dam_small"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=25.0)
+    ap.add_argument("--ref-max-steps", type=int, default=5)
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl" if args.impl == "b200" else "gloo",
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    torch.cuda.set_device(local)
+    import mphexplicit_b200 as M
+    sc = make_scene(args, rank)
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim, mode=args.mode)
+    s.step(max(args.warmup, 3))
+    s.synchronize()
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    # ---- device-resident timed region ----------------------------------
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    gpu_index = local
+    cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if cvd and "," not in cvd and cvd.isdigit():
+        gpu_index = int(cvd)
+    s.profile(True)
+    l0 = s.launch_count()
+    info0 = s.info()
+    with ClockSampler(gpu_index) as clk:
+        ev0.record(stream)
+        s.step(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launch_count() - l0
+    prof = s.profile_read()
+    s.profile(False)
+    info1 = s.info()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n_fluid, n_all = sc.n_fluid, sc.n
+    value = n_fluid * args.steps * world / (ms / 1e3)
+
+    # roofline of the dominant kernel
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (nl, tot_ms) = dom
+    avg_s = tot_ms / nl / 1e3
+    peak, peak_kind = measured_peaks()
+    algo = ALGO_BYTES.get(name, 0.0) * n_all
+    achieved = algo / avg_s / 1e9
+    roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": ncu_traffic(name), "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3,
+            "kernels_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    ke = max(1, args.e2e_steps)
+    hx = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
+    s.get_xv(hx, hv)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(ke):
+        s.set_state(hx, hv)
+        s.step(1)
+        s.get_xv(hx, hv)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    e2e_ms = max(ev0.elapsed_time(ev1), e2e_wall * 1e3)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": n_fluid * ke * world / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes), "d2h_bytes_per_step": int(hx.nbytes + hv.nbytes),
+           "steps": ke}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(sc, args.ref_seconds, args.ref_max_steps)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32/f64",
+                "data": "synthetic (seeded generator)",
+                "config": {"workload": workload_name(sc), "mode": args.mode,
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (%.2f GB device state)" % (n_all * 260 / 1e9),
+                           "rebuilds_in_timed_region": info1["rebuild_count"] - info0["rebuild_count"],
+                           "updates_all_particles_per_s": n_all * args.steps * world / (ms / 1e3)},
+                "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

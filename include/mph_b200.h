@@ -1,0 +1,249 @@
+/*
+ * mph_b200.h — C ABI of the B200 (sm_100a) MPH-WC explicit time step.
+ *
+ * The reference solver (Masahiro-Kondo-AIST/MphExplicit) is one C++ program whose
+ * state lives in file-scope statics of source/main.cpp and whose step is the body
+ * of the while loop at source/main.cpp:374-452.  It has no library interface; the
+ * replaceable units are its file readers/writers, its set-up routines and the
+ * per-step call sequence.  Each entry point below names the reference routine(s)
+ * it replaces.  All entry points:
+ *   - take plain host pointers and sizes (no device or framework types);
+ *   - return an int status (MPH_OK == 0, negative on error) and never exit();
+ *   - copy what they are given: the caller owns host buffers, the library owns
+ *     device memory.
+ * A context is used by one host thread at a time.  Work is ordered on one CUDA
+ * stream per context; functions that return host data synchronise that stream.
+ *
+ * Particle arrays are "double[n][3]" (x,y,z per particle) as in the reference
+ * (DIM is 3 even in 2-D, main.cpp:40).  Types 0/1 are fluid, 2/3 are wall
+ * (main.cpp:43-47).
+ */
+#ifndef MPH_B200_H
+#define MPH_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPH_TYPE_COUNT 4
+
+/* ---- status codes ---------------------------------------------------- */
+#define MPH_OK               0
+#define MPH_ERR_ARG         -1   /* invalid argument                        */
+#define MPH_ERR_IO          -2   /* file could not be opened / parsed       */
+#define MPH_ERR_CUDA        -3   /* CUDA runtime error                      */
+#define MPH_ERR_CAPACITY    -4   /* a device-side capacity was exceeded     */
+#define MPH_ERR_DEVICE      -5   /* device-side error flag was raised       */
+#define MPH_ERR_NONFINITE   -6   /* NaN/Inf detected in the particle state  */
+#define MPH_ERR_STATE       -7   /* call not valid in the context's state   */
+#define MPH_ERR_NOMEM       -8   /* host or device allocation failed        */
+#define MPH_ERR_GEOMETRY    -9   /* cell grid incompatible with the radius  */
+
+/* ---- step forms ------------------------------------------------------ */
+/* Plain FP64 in the reference's operation order: bitonic cell sort, Verlet
+ * neighbour list in the reference order, every pair sum in list order, no FMA
+ * contraction.  Results are bit-identical to the reference's x86-64 build. */
+#define MPH_MODE_FP64     0
+/* FP32 pair arithmetic on cell-relative coordinates with compensated
+ * per-particle sums; FP64 position/velocity integration; counting-sort cell
+ * lists rebuilt every step (no stored neighbour list). */
+#define MPH_MODE_MIXED    1
+
+/* ---- parameters read from the *.data file (main.cpp:489-539) --------- */
+typedef struct mph_params {
+    double dt;                                   /* Dt                       */
+    double output_interval;                      /* OutputInterval           */
+    double vtk_output_interval;                  /* VtkOutputInterval        */
+    double end_time;                             /* EndTime                  */
+    double radius_ratio_a;                       /* RadiusRatioA (= ratio G) */
+    double radius_ratio_p;                       /* RadiusRatioP             */
+    double radius_ratio_v;                       /* RadiusRatioV             */
+    double density[MPH_TYPE_COUNT];
+    double bulk_modulus[MPH_TYPE_COUNT];
+    double bulk_viscosity[MPH_TYPE_COUNT];
+    double shear_viscosity[MPH_TYPE_COUNT];
+    double surface_tension[MPH_TYPE_COUNT];
+    double interaction_ratio[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
+    double gravity[3];
+    double wall_center[MPH_TYPE_COUNT][3];       /* rows 2 and 3 are used    */
+    double wall_velocity[MPH_TYPE_COUNT][3];
+    double wall_omega[MPH_TYPE_COUNT][3];
+} mph_params;
+
+/* ---- first two lines of a *.grid / *.prof file (main.cpp:549-557) ---- */
+typedef struct mph_grid_header {
+    double time;
+    int    particle_count;
+    double particle_spacing;
+    double domain_min[3];
+    double domain_max[3];
+} mph_grid_header;
+
+/* ---- derived constants (initializeWeight/Fluid/Domain, main.cpp:836-1084) */
+typedef struct mph_constants {
+    int    dim;
+    double particle_volume;
+    double radius_a, radius_g, radius_p, radius_v, max_radius;
+    double swa, swg, swp, swv, n0a, n0p, r2g;
+    int    n0a_count, n0p_count;
+    double cof_k, cof_a[MPH_TYPE_COUNT];
+    double domain_width[3];
+    int    cell_count[3];
+    int    total_cell_count;
+    double cell_width[3];
+    double wall_rotation[MPH_TYPE_COUNT][3][3];
+} mph_constants;
+
+/* ---- run-time counters of a context --------------------------------- */
+typedef struct mph_info {
+    int       particle_count;
+    int       fluid_particle_begin, fluid_particle_end;   /* sorted order      */
+    int       wall_particle_begin, wall_particle_end;
+    long long neighbor_ind_count;     /* NeighborIndCount (FP64 form)          */
+    int       max_neighbor_count;     /* longest neighbour list                */
+    int       neighbor_capacity;      /* allocated list length per particle    */
+    long long step;                   /* steps taken since mph_create          */
+    long long rebuild_count;          /* neighbour rebuilds inside mph_step    */
+    double    time;                   /* Time                                  */
+    int       mode;
+} mph_info;
+
+typedef struct mph_ctx mph_ctx;
+
+/* Zero/neutral parameters, matching the reference statics before
+ * readDataFile runs (Dt = 1e100, everything else 0; main.cpp:56-211). */
+int mph_params_defaults(mph_params* p);
+
+/* Parse a *.data file.  Replaces readDataFile (main.cpp:489-539): same keys,
+ * same sscanf patterns, '#' lines skipped, unknown lines counted in
+ * *invalid_lines (may be NULL).  Returns MPH_ERR_IO if the file cannot be
+ * opened (the reference would crash in fclose(NULL)). */
+int mph_read_data_file(const char* path, mph_params* p, int* invalid_lines);
+
+/* Read the two header lines of a *.grid / *.prof file (main.cpp:549-557). */
+int mph_read_grid_header(const char* path, mph_grid_header* h);
+
+/* Read a *.grid / *.prof file into caller arrays of `capacity` particles.
+ * Replaces the parsing part of readGridFile (main.cpp:541-640).  A file with
+ * fewer particle lines than its header announces returns MPH_ERR_IO (the
+ * reference silently leaves the rest uninitialised). */
+int mph_read_grid_file(const char* path, mph_grid_header* h, int capacity,
+                       int* type, double* xyz, double* vel);
+
+/* Write a *.grid / *.prof file.  Same format as writeProfFile
+ * (main.cpp:672-696) and the generator (generator/generator.cpp:197-217 uses
+ * "%lf" for time; this writer uses the solver's "%e"). */
+int mph_write_grid_file(const char* path, const mph_grid_header* h,
+                        const int* type, const double* xyz, const double* vel);
+
+/* Compute the derived constants without creating a context (initializeWeight,
+ * initializeFluid's CofK/CofA, initializeWall, initializeDomain). dim is 2 or 3. */
+int mph_compute_constants(const mph_params* p, const mph_grid_header* h, int dim,
+                          mph_constants* c);
+
+/* Create a context on the current CUDA device: copy the particles in, run the
+ * set-up (main.cpp:330-333), the initial cell sort and neighbour list
+ * (main.cpp:358-359) and the initial densities (main.cpp:362-364).
+ * `type`, `xyz`, `vel` are in file order. */
+int mph_create(const mph_params* p, const mph_grid_header* h, int dim, int mode,
+               const int* type, const double* xyz, const double* vel,
+               mph_ctx** out);
+
+/* Advance nsteps explicit steps: the loop body main.cpp:386-431 plus
+ * Time += Dt (main.cpp:449).  No file output.  Enqueued on the context's
+ * stream; the neighbour-rebuild test reads one flag per step. */
+int mph_step(mph_ctx* ctx, int nsteps);
+
+/* Wait for the context's stream and report any device-side error flag. */
+int mph_synchronize(mph_ctx* ctx);
+
+int mph_get_info(mph_ctx* ctx, mph_info* info);
+int mph_get_constants(mph_ctx* ctx, mph_constants* c);
+
+/* Copy the current particle state to host arrays, in the context's current
+ * (cell-sorted) order, as the reference's arrays are after a step.  Any pointer
+ * may be NULL.  particle_index[i] is the file-order id of slot i
+ * (ParticleIndex, main.cpp:75).  virial_pressure is valid after
+ * mph_compute_virial. */
+int mph_get_state(mph_ctx* ctx, int* particle_index, int* type,
+                  double* xyz, double* vel, double* force, int* neighbor_count,
+                  double* density_a, double* vol_strain_p, double* virial_pressure);
+
+/* Overwrite positions and velocities (same sorted order as mph_get_state).
+ * Used by callers that keep the state on the host between steps. */
+int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel);
+
+/* Secondary per-particle fields in sorted order (any pointer may be NULL):
+ * DivergenceP, PressureP, PressureA, GravityCenter[3]. */
+int mph_get_fields(mph_ctx* ctx, double* divergence_p, double* pressure_p,
+                   double* pressure_a, double* gravity_center);
+
+/* Cell data of the last rebuild (FP64 form): CellIndex per sorted slot and
+ * the per-cell fluid/wall particle ranges (main.cpp:1160-1247).  Arrays of
+ * particle_count and total_cell_count entries; any pointer may be NULL. */
+int mph_get_cells(mph_ctx* ctx, int* cell_index, int* fluid_begin, int* fluid_end,
+                  int* wall_begin, int* wall_end);
+
+/* The neighbour list of the last rebuild in CSR form (NeighborPtr /
+ * NeighborInd, main.cpp:1452-1585): ptr has particle_count+1 entries, ind has
+ * neighbor_ind_count entries.  FP64 form only. */
+int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long long ind_capacity);
+
+/* Virial stress and pressure at particles (calculateVirialStressAtParticle,
+ * main.cpp:2057-2302), computed on the device from the current state. */
+int mph_compute_virial(mph_ctx* ctx);
+
+/* Output files in the reference formats and in sorted order:
+ * writeVtkFile (main.cpp:698-834) and writeProfFile (main.cpp:672-696). */
+int mph_write_vtk(mph_ctx* ctx, const char* path);
+int mph_write_prof(mph_ctx* ctx, const char* path);
+
+/* writeVtkFile (main.cpp:698-834) from caller host arrays of n particles
+ * (no context needed): same text, same field order, same float casts. */
+int mph_write_vtk_arrays(const char* path, int n, const int* type, const double* xyz,
+                         const double* vel, const double* force, const int* neighbor_count,
+                         const double* density_a, const double* vol_strain_p,
+                         const double* virial_pressure);
+
+/* Mass, momentum and kinetic energy of the fluid, summed in FP64 on the
+ * device (diagnostic of the mixed form).  out[0]=mass, out[1..3]=momentum,
+ * out[4]=kinetic energy. */
+int mph_conserved_sums(mph_ctx* ctx, double out[5]);
+
+/* ---- measurement hooks (no reference counterpart: the reference only has
+ * clock() totals, main.cpp:287-288, 456-465) ---------------------------- */
+
+/* The CUDA stream (cudaStream_t) all work of ctx is ordered on, so a caller
+ * can record its own CUDA events around mph_step. */
+void* mph_stream(mph_ctx* ctx);
+
+/* Kernels launched by ctx since mph_create. */
+long long mph_launch_count(mph_ctx* ctx);
+
+typedef struct mph_kernel_stat {
+    char      name[32];
+    long long launches;
+    double    total_ms;   /* sum of CUDA-event durations on the ctx stream */
+} mph_kernel_stat;
+
+/* enable != 0: from now on bracket every kernel launch with CUDA events on
+ * the context's stream (statistics are reset).  enable == 0: stop. */
+int mph_profile_enable(mph_ctx* ctx, int enable);
+
+/* Synchronise and return the per-kernel statistics gathered since the last
+ * mph_profile_enable(ctx, 1); *count receives the number of kernel names. */
+int mph_profile_read(mph_ctx* ctx, mph_kernel_stat* out, int capacity, int* count);
+
+/* Last error message of ctx (or of the calling thread if ctx is NULL). */
+int mph_last_error(mph_ctx* ctx, char* buf, int len);
+
+void mph_destroy(mph_ctx* ctx);
+
+/* Library version string. */
+const char* mph_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPH_B200_H */

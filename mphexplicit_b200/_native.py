@@ -1,0 +1,181 @@
+"""ctypes view of the C ABI declared in include/mph_b200.h.
+
+The structures below mirror the header field for field.  ``load()`` opens the
+in-tree ``libmph_b200.so``; there is no fallback: if the library is missing the
+import of the solver fails with the build command in the message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+TYPE_COUNT = 4
+
+MPH_OK = 0
+MPH_ERR_ARG = -1
+MPH_ERR_IO = -2
+MPH_ERR_CUDA = -3
+MPH_ERR_CAPACITY = -4
+MPH_ERR_DEVICE = -5
+MPH_ERR_NONFINITE = -6
+MPH_ERR_STATE = -7
+MPH_ERR_NOMEM = -8
+MPH_ERR_GEOMETRY = -9
+
+MODE_FP64 = 0
+MODE_MIXED = 1
+
+_D4 = C.c_double * TYPE_COUNT
+_D44 = (C.c_double * TYPE_COUNT) * TYPE_COUNT
+_D3 = C.c_double * 3
+_D43 = (C.c_double * 3) * TYPE_COUNT
+
+
+class Params(C.Structure):
+    """mph_params: the keys of the reference's *.data file (main.cpp:489-539)."""
+
+    _fields_ = [
+        ("dt", C.c_double),
+        ("output_interval", C.c_double),
+        ("vtk_output_interval", C.c_double),
+        ("end_time", C.c_double),
+        ("radius_ratio_a", C.c_double),
+        ("radius_ratio_p", C.c_double),
+        ("radius_ratio_v", C.c_double),
+        ("density", _D4),
+        ("bulk_modulus", _D4),
+        ("bulk_viscosity", _D4),
+        ("shear_viscosity", _D4),
+        ("surface_tension", _D4),
+        ("interaction_ratio", _D44),
+        ("gravity", _D3),
+        ("wall_center", _D43),
+        ("wall_velocity", _D43),
+        ("wall_omega", _D43),
+    ]
+
+
+class GridHeader(C.Structure):
+    """mph_grid_header: first two lines of a *.grid / *.prof file."""
+
+    _fields_ = [
+        ("time", C.c_double),
+        ("particle_count", C.c_int),
+        ("particle_spacing", C.c_double),
+        ("domain_min", _D3),
+        ("domain_max", _D3),
+    ]
+
+
+class Constants(C.Structure):
+    """mph_constants: derived set-up values (main.cpp:836-1084)."""
+
+    _fields_ = [
+        ("dim", C.c_int),
+        ("particle_volume", C.c_double),
+        ("radius_a", C.c_double),
+        ("radius_g", C.c_double),
+        ("radius_p", C.c_double),
+        ("radius_v", C.c_double),
+        ("max_radius", C.c_double),
+        ("swa", C.c_double),
+        ("swg", C.c_double),
+        ("swp", C.c_double),
+        ("swv", C.c_double),
+        ("n0a", C.c_double),
+        ("n0p", C.c_double),
+        ("r2g", C.c_double),
+        ("n0a_count", C.c_int),
+        ("n0p_count", C.c_int),
+        ("cof_k", C.c_double),
+        ("cof_a", _D4),
+        ("domain_width", _D3),
+        ("cell_count", C.c_int * 3),
+        ("total_cell_count", C.c_int),
+        ("cell_width", _D3),
+        ("wall_rotation", ((C.c_double * 3) * 3) * TYPE_COUNT),
+    ]
+
+
+class Info(C.Structure):
+    """mph_info: run-time counters of a context."""
+
+    _fields_ = [
+        ("particle_count", C.c_int),
+        ("fluid_particle_begin", C.c_int),
+        ("fluid_particle_end", C.c_int),
+        ("wall_particle_begin", C.c_int),
+        ("wall_particle_end", C.c_int),
+        ("neighbor_ind_count", C.c_longlong),
+        ("max_neighbor_count", C.c_int),
+        ("neighbor_capacity", C.c_int),
+        ("step", C.c_longlong),
+        ("rebuild_count", C.c_longlong),
+        ("time", C.c_double),
+        ("mode", C.c_int),
+    ]
+
+
+class KernelStat(C.Structure):
+    """mph_kernel_stat: per-kernel launches and CUDA-event time."""
+
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double)]
+
+
+# every symbol the header declares, with its ctypes signature
+_P = C.c_void_p
+_I = C.c_int
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+SIGNATURES = {
+    "mph_params_defaults": (_I, [C.POINTER(Params)]),
+    "mph_read_data_file": (_I, [C.c_char_p, C.POINTER(Params), _ip]),
+    "mph_read_grid_header": (_I, [C.c_char_p, C.POINTER(GridHeader)]),
+    "mph_read_grid_file": (_I, [C.c_char_p, C.POINTER(GridHeader), _I, _ip, _dp, _dp]),
+    "mph_write_grid_file": (_I, [C.c_char_p, C.POINTER(GridHeader), _ip, _dp, _dp]),
+    "mph_compute_constants": (_I, [C.POINTER(Params), C.POINTER(GridHeader), _I, C.POINTER(Constants)]),
+    "mph_create": (_I, [C.POINTER(Params), C.POINTER(GridHeader), _I, _I, _ip, _dp, _dp, C.POINTER(_P)]),
+    "mph_step": (_I, [_P, _I]),
+    "mph_synchronize": (_I, [_P]),
+    "mph_get_info": (_I, [_P, C.POINTER(Info)]),
+    "mph_get_constants": (_I, [_P, C.POINTER(Constants)]),
+    "mph_get_state": (_I, [_P, _ip, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp]),
+    "mph_set_state": (_I, [_P, _dp, _dp]),
+    "mph_get_fields": (_I, [_P, _dp, _dp, _dp, _dp]),
+    "mph_get_cells": (_I, [_P, _ip, _ip, _ip, _ip, _ip]),
+    "mph_get_neighbors": (_I, [_P, C.POINTER(C.c_longlong), _ip, C.c_longlong]),
+    "mph_compute_virial": (_I, [_P]),
+    "mph_write_vtk": (_I, [_P, C.c_char_p]),
+    "mph_write_prof": (_I, [_P, C.c_char_p]),
+    "mph_write_vtk_arrays": (_I, [C.c_char_p, _I, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp]),
+    "mph_conserved_sums": (_I, [_P, _dp]),
+    "mph_stream": (_P, [_P]),
+    "mph_launch_count": (C.c_longlong, [_P]),
+    "mph_profile_enable": (_I, [_P, _I]),
+    "mph_profile_read": (_I, [_P, C.POINTER(KernelStat), _I, _ip]),
+    "mph_last_error": (_I, [_P, C.c_char_p, _I]),
+    "mph_destroy": (None, [_P]),
+    "mph_version": (C.c_char_p, []),
+}
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libmph_b200.so")
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Open the in-tree sm_100a library (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing; build it with `make -C {os.path.join(PKG_DIR, 'csrc')}` "
+            "or `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib

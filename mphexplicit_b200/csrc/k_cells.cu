@@ -1,0 +1,280 @@
+// k_cells.cu — cell assignment, bitonic cell sort, per-cell ranges, reorder and
+// the Verlet neighbour list of the FP64 form (sm_100a).
+//
+// This is integer/index work plus the FP64 distance test of the list build.
+// The results are bit-exact against the reference:
+//   * cell index:      main.cpp:1115-1133 (same floor/modulo expressions);
+//   * sort:            the reference's bitonic compare-exchange network
+//                      (main.cpp:1137-1158), pass for pass, so ties inside a
+//                      cell end in the same order and the permutation matches;
+//   * per-cell ranges: main.cpp:1160-1247 (begin/end equal the number of sorted
+//                      keys below each key value, found here by binary search);
+//   * neighbour list:  main.cpp:1329-1596, same stencil order, self included,
+//                      wall particles without a fluid neighbour get no list.
+// Compiled with -fmad=false so the distance test is not FMA-contracted.
+#include "mph_internal.h"
+
+namespace mph {
+
+namespace {
+
+constexpr int kLogLocal = 12;               // 4096 keys per shared-memory block
+constexpr int kLocal = 1 << kLogLocal;
+constexpr int kSortThreads = 1024;
+
+__device__ __forceinline__ double omod(double x, double w) { return x - w * floor(x / w); }
+
+// Mod(x,w) of main.cpp:70.  When 0 <= x < 0.75 w the quotient rounds below 1,
+// floor gives +0 and the expression returns x exactly; skip the division then.
+__device__ __forceinline__ double omod_fast(double x, double w) {
+    return (x >= 0.0 && x < 0.75 * w) ? x : omod(x, w);
+}
+
+__device__ __forceinline__ int cell_id(const SimConst& c, int ix, int iy, int iz) {  // main.cpp:96-100
+    return ((ix % c.cc[0] + c.cc[0]) % c.cc[0]) * c.cc[1] * c.cc[2] +
+           ((iy % c.cc[1] + c.cc[1]) % c.cc[1]) * c.cc[2] + ((iz % c.cc[2] + c.cc[2]) % c.cc[2]);
+}
+
+__global__ void k_cell_index(SimConst c, const double4* __restrict__ pos, const int* __restrict__ type,
+                             int* __restrict__ keys, int* __restrict__ vals) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.pow2) return;
+    if (i < c.n) {
+        const double4 p = pos[i];
+        const int cx = ((int)floor((p.x - c.dmin[0]) / c.cell_width[0])) % c.cc[0];
+        const int cy = ((int)floor((p.y - c.dmin[1]) / c.cell_width[1])) % c.cc[1];
+        const int cz = ((int)floor((p.z - c.dmin[2]) / c.cell_width[2])) % c.cc[2];
+        int id = cell_id(c, cx, cy, cz);
+        const int t = type[i];
+        if (t >= 2 && t < 4) id += c.tot;
+        keys[i] = id;
+        vals[i] = i;
+    } else {
+        keys[i] = 2 * c.tot;
+        vals[i] = c.n;
+    }
+}
+
+// One compare-exchange of pass (m, dist): element i (bit log2(dist) clear) and
+// i|dist; ascending when bit m+1 of i is clear (main.cpp:1146-1148).
+__device__ __forceinline__ void cmpx(int* k, int* v, int a, int b, bool up) {
+    const int ka = k[a], kb = k[b];
+    if ((ka > kb) == up) {
+        const int va = v[a], vb = v[b];
+        k[a] = kb; k[b] = ka;
+        v[a] = vb; v[b] = va;
+    }
+}
+
+// All passes whose distance is below the block size, for main-stage m in
+// [m_begin, m_end); for each m the sub-stages with dist < block run here.
+// Block b owns keys [b*L, (b+1)*L).
+__global__ void __launch_bounds__(kSortThreads)
+k_bitonic_local(int* __restrict__ keys, int* __restrict__ vals, int L, int logL, int m_begin, int m_end) {
+    __shared__ int sk[kLocal];
+    __shared__ int sv[kLocal];
+    const int base = blockIdx.x * L;
+    for (int t = threadIdx.x; t < L; t += blockDim.x) {
+        sk[t] = keys[base + t];
+        sv[t] = vals[base + t];
+    }
+    __syncthreads();
+    const int half = L >> 1;
+    for (int m = m_begin; m < m_end; ++m) {
+        // sub-stages with dist = 2^(m-k) < L, i.e. log2(dist) <= min(m, logL-1)
+        const int top = m < logL - 1 ? m : logL - 1;
+        for (int ld = top; ld >= 0; --ld) {
+            const int dist = 1 << ld;
+            for (int t = threadIdx.x; t < half; t += blockDim.x) {
+                const int i = ((t >> ld) << (ld + 1)) | (t & (dist - 1));
+                const bool up = (((base + i) >> m) & 2) == 0;
+                cmpx(sk, sv, i, i | dist, up);
+            }
+            __syncthreads();
+        }
+    }
+    for (int t = threadIdx.x; t < L; t += blockDim.x) {
+        keys[base + t] = sk[t];
+        vals[base + t] = sv[t];
+    }
+}
+
+// One pass with dist >= block size, one pair per thread.
+__global__ void k_bitonic_global(int* __restrict__ keys, int* __restrict__ vals, int npairs, int m, int ld) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= npairs) return;
+    const int dist = 1 << ld;
+    const int i = ((t >> ld) << (ld + 1)) | (t & (dist - 1));
+    const bool up = ((i >> m) & 2) == 0;
+    cmpx(keys, vals, i, i | dist, up);
+}
+
+// cellstart[b] = number of sorted keys below b, b in [0, 2*tot].  These are
+// the reference's CellFluidParticleBegin/End (b < tot) and
+// CellWallParticleBegin/End (b >= tot) after its prefix sum (main.cpp:1191-1247).
+__global__ void k_cell_ranges(const int* __restrict__ keys, int n, int nb, int* __restrict__ cellstart) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    cellstart[b] = lo;
+}
+
+// Gather by the sorted CellParticle (main.cpp:1262-1325); the snapshot of the
+// positions for the rebuild test is taken here (main.cpp:1587-1595: the
+// positions do not change between the reorder and the end of the build).
+__global__ void k_reorder(int n, const int* __restrict__ vals, const int* __restrict__ pidx_in,
+                          const int* __restrict__ type_in, const double4* __restrict__ pos_in,
+                          const double4* __restrict__ vel_in, int* __restrict__ pidx_out,
+                          int* __restrict__ type_out, double4* __restrict__ pos_out,
+                          double4* __restrict__ vel_out, double4* __restrict__ snap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = vals[i];
+    pidx_out[i] = pidx_in[s];
+    type_out[i] = type_in[s];
+    const double4 p = pos_in[s];
+    pos_out[i] = p;
+    snap[i] = p;
+    vel_out[i] = vel_in[s];
+}
+
+// Neighbour list, one thread per particle (main.cpp:1329-1585).  The count and
+// the fill of the reference are one pass here: entries go to a column-major
+// [cap][n] table; a list longer than cap is still counted, raises
+// DEVFLAG_NEIGHBOR_OVERFLOW and the host rebuilds with a larger table.
+__global__ void __launch_bounds__(256)
+k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restrict__ keys,
+                const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist,
+                int cap, StepScalars* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const int ci = keys[i];
+    const int icx = (ci / (c.cc[1] * c.cc[2])) % c.tot;     // main.cpp:1356-1358
+    const int icy = (ci / c.cc[2]) % c.cc[1];
+    const int icz = ci % c.cc[2];
+    int jc[3][3];
+    const int ic[3] = {icx, icy, icz};
+    int jmin[3], w[3];
+    for (int d = 0; d < 3; ++d) {
+        const int r = c.range[d];
+        w[d] = 2 * r + 1;
+        for (int j = 0; j < w[d]; ++j) jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
+        const int b = (2 * r) - (ic[d] + r) % c.cc[d];       // main.cpp:1376-1381
+        jmin[d] = b > 0 ? b : 0;
+    }
+    int cells[27];
+    int nc = 0;
+    for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+        for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+            for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz)
+                cells[nc++] = cell_id(c, jc[0][jx % w[0]], jc[1][jy % w[1]], jc[2][jz % w[2]]);
+    const double4 pi = pos[i];
+    const int wall_begin = cellstart[c.tot], wall_end = cellstart[2 * c.tot];
+    const size_t n = (size_t)c.n;
+    int cnt = 0;
+    for (int kind = 0; kind < 2; ++kind) {
+        if (kind == 1 && wall_begin <= i && i < wall_end && cnt == 0) break;  // main.cpp:1416
+        const int off = kind ? c.tot : 0;
+        for (int k = 0; k < nc; ++k) {
+            const int b = cellstart[cells[k] + off], e = cellstart[cells[k] + off + 1];
+            for (int j = b; j < e; ++j) {
+                const double4 pj = pos[j];
+                const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+                const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+                const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                if (r2 <= c.rm2) {
+                    if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
+                    cnt++;
+                }
+            }
+        }
+    }
+    ncount[i] = cnt;
+    atomicMax(&scal->max_neighbors, cnt);
+    if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+}
+
+__global__ void k_pack3(int n, const double4* __restrict__ src, double* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 p = src[i];
+    dst[3 * (size_t)i + 0] = p.x;
+    dst[3 * (size_t)i + 1] = p.y;
+    dst[3 * (size_t)i + 2] = p.z;
+}
+
+__global__ void k_unpack3(int n, const double* __restrict__ src, double4* __restrict__ dst,
+                          const int* __restrict__ type) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double w = type ? (double)type[i] : 0.0;
+    dst[i] = make_double4(src[3 * (size_t)i], src[3 * (size_t)i + 1], src[3 * (size_t)i + 2], w);
+}
+
+inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_cell_index(const SimConst& c, const double4* pos, const int* type, int* keys, int* vals,
+                       cudaStream_t s) {
+    k_cell_index<<<blocks(c.pow2, 256), 256, 0, s>>>(c, pos, type, keys, vals);
+}
+
+// The reference's network (main.cpp:1137-1158): for m in [0, log2 P), k in [0, m],
+// dist = 2^(m-k).  Passes with dist below the shared-memory block run inside
+// k_bitonic_local; the others one launch each.  Same passes, same order.
+int launch_bitonic_sort(const SimConst& c, int* keys, int* vals, cudaStream_t s) {
+    const int P = c.pow2;
+    int logP = 0;
+    while ((1 << logP) < P) ++logP;
+    if (logP == 0) return 0;
+    const int logL = logP < kLogLocal ? logP : kLogLocal;
+    const int L = 1 << logL;
+    const int nblk = P / L;
+    const int thr = (L / 2) < kSortThreads ? (L / 2) : kSortThreads;
+    int launches = 0;
+    // every main stage m < logL is entirely local
+    k_bitonic_local<<<nblk, thr, 0, s>>>(keys, vals, L, logL, 0, logL);
+    ++launches;
+    for (int m = logL; m < logP; ++m) {
+        for (int ld = m; ld >= logL; --ld) {
+            k_bitonic_global<<<blocks(P / 2, 256), 256, 0, s>>>(keys, vals, P / 2, m, ld);
+            ++launches;
+        }
+        k_bitonic_local<<<nblk, thr, 0, s>>>(keys, vals, L, logL, m, m + 1);
+        ++launches;
+    }
+    return launches;
+}
+
+void launch_cell_ranges(const SimConst& c, const int* keys, int* cellstart, cudaStream_t s) {
+    const int nb = 2 * c.tot + 1;
+    k_cell_ranges<<<blocks(nb, 256), 256, 0, s>>>(keys, c.n, nb, cellstart);
+}
+
+void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, const int* type_in,
+                    const double4* pos_in, const double4* vel_in, int* pidx_out, int* type_out,
+                    double4* pos_out, double4* vel_out, double4* snap, cudaStream_t s) {
+    k_reorder<<<blocks(c.n, 256), 256, 0, s>>>(c.n, vals, pidx_in, type_in, pos_in, vel_in, pidx_out,
+                                               type_out, pos_out, vel_out, snap);
+}
+
+void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys, const int* cellstart,
+                          int* ncount, int* nlist, int cap, StepScalars* scal, cudaStream_t s) {
+    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, keys, cellstart, ncount, nlist, cap, scal);
+}
+
+void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s) {
+    k_pack3<<<blocks(n, 256), 256, 0, s>>>(n, src, dst);
+}
+
+void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s) {
+    k_unpack3<<<blocks(n, 256), 256, 0, s>>>(n, src, dst, type);
+}
+
+}  // namespace mph

@@ -1,0 +1,485 @@
+// k_fp64.cu — the plain FP64 MPH-WC step on sm_100a, bit-exact against the
+// reference's x86-64 build.
+//
+// The reference runs eight neighbour sweeps per step (main.cpp:1665-1985).
+// Here they are two, one thread per particle, list order kept:
+//   sweep A = DensityA + GravityCenter + DensityP + DivergenceP
+//             (four independent sums over the same list) and, in the epilogue,
+//             PhysicalCoefficients + PressureP value + PressureA value;
+//   sweep B = PressureP + PressureA + DiffuseInterface + ViscosityV forces,
+//             each in its own accumulator, added to Force in the reference's
+//             order, then Gravity + Acceleration (velocity double-buffered).
+// plus one per-particle kernel for Convection + Wall + PeriodicBoundary +
+// the rebuild test.  Every FP expression keeps the reference's association
+// order; the file is compiled with -fmad=false and uses IEEE division and
+// square root, so each operation rounds exactly as on the CPU.
+#include "mph_internal.h"
+
+namespace mph {
+
+namespace {
+
+__device__ __forceinline__ double omod(double x, double w) { return x - w * floor(x / w); }
+
+// Mod(x,w), main.cpp:70.  When 0 <= x < 0.75 w the rounded quotient is below 1,
+// floor gives +0 and x - w*0 == x exactly: the division is skipped then.
+__device__ __forceinline__ double omod_fast(double x, double w) {
+    return (x >= 0.0 && x < 0.75 * w) ? x : omod(x, w);
+}
+
+// Minimum-image displacement x_j - x_i (main.cpp:1680 and every sweep).
+__device__ __forceinline__ void disp(const SimConst& c, const double4& pi, const double4& pj, double* x) {
+    x[0] = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+    x[1] = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+    x[2] = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+}
+
+// Kernel shapes, main.cpp:214-284, with q = r/h computed by division.
+__device__ __forceinline__ double f_wa(const SimConst& c, double r) {
+    const double q = r / c.ra;
+    return ((c.ca * q) * (1.0 - q)) * (1.0 - q);
+}
+__device__ __forceinline__ double f_dwadr(const SimConst& c, double r) {
+    const double q = r / c.ra;
+    return ((c.ca * (1.0 - q)) * (1.0 - 3.0 * q)) * c.inv_ra;
+}
+__device__ __forceinline__ double f_wg(const SimConst& c, double r) {
+    const double q = r / c.rg;
+    return c.cg * ((1.0 - q) * (1.0 - q));
+}
+__device__ __forceinline__ double f_dwgdr(const SimConst& c, double r) {
+    const double q = r / c.rg;
+    return c.cg * (c.m2_rg * (1.0 - q));
+}
+__device__ __forceinline__ double f_wp(const SimConst& c, double r) {
+    const double q = r / c.rp;
+    return c.cp * ((1.0 - q) * (1.0 - q));
+}
+__device__ __forceinline__ double f_dwpdr(const SimConst& c, double r) {
+    const double q = r / c.rp;
+    return c.cp * (c.m2_rp * (1.0 - q));
+}
+__device__ __forceinline__ double f_dwvdr(const SimConst& c, double r) {
+    const double q = r / c.rv;
+    return c.cv * (c.m2_rv * (1.0 - q));
+}
+
+__device__ __forceinline__ int type_of(const double4& p) { return (int)p.w; }
+
+// Convection (main.cpp:1605-1615), Wall (2013-2043), PeriodicBoundary
+// (2306-2317) and the displacement maximum of neighborCalculation (1086-1100).
+__global__ void __launch_bounds__(256)
+k_move(SimConst c, const int* __restrict__ cellstart, double4* __restrict__ pos, double4* __restrict__ vel,
+       const double4* __restrict__ snap, const double* __restrict__ wall_center, StepScalars* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s2 = 0.0;
+    if (i < c.n) {
+        const int nf = cellstart[c.tot], we = cellstart[2 * c.tot];
+        double4 p = pos[i];
+        if (i < nf) {
+            const double4 v = vel[i];
+            p.x += v.x * c.dt;
+            p.y += v.y * c.dt;
+            p.z += v.z * c.dt;
+        } else if (i < we) {
+            const int t = type_of(p);
+            const double* C = wall_center + 3 * t;
+            const double (*R)[3] = c.wall_rot[t];
+            const double* W = c.wall_omega[t];
+            const double* U = c.wall_velocity[t];
+            double r0 = p.x - C[0], r1 = p.y - C[1], r2 = p.z - C[2];
+            r0 = R[0][0] * r0 + R[0][1] * r1 + R[0][2] * r2;   // in place, as main.cpp:2033-2035
+            r1 = R[1][0] * r0 + R[1][1] * r1 + R[1][2] * r2;
+            r2 = R[2][0] * r0 + R[2][1] * r1 + R[2][2] * r2;
+            double4 v = vel[i];
+            v.x = W[1] * r2 - W[2] * r1 + U[0];
+            v.y = W[2] * r0 - W[0] * r2 + U[1];
+            v.z = W[0] * r1 - W[1] * r0 + U[2];
+            vel[i] = v;
+            p.x = r0 + C[0] + U[0] * c.dt;
+            p.y = r1 + C[1] + U[1] * c.dt;
+            p.z = r2 + C[2] + U[2] * c.dt;
+        }
+        p.x = omod_fast(p.x - c.dmin[0], c.width[0]) + c.dmin[0];
+        p.y = omod_fast(p.y - c.dmin[1], c.width[1]) + c.dmin[1];
+        p.z = omod_fast(p.z - c.dmin[2], c.width[2]) + c.dmin[2];
+        pos[i] = p;
+        const double4 q = snap[i];
+        double d[3];
+        d[0] = omod_fast(p.x - q.x + c.half_width[0], c.width[0]) - c.half_width[0];
+        d[1] = omod_fast(p.y - q.y + c.half_width[1], c.width[1]) - c.half_width[1];
+        d[2] = omod_fast(p.z - q.z + c.half_width[2], c.width[2]) - c.half_width[2];
+        s2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        if (!(s2 > 0.0)) s2 = 0.0;  // a NaN never wins the reference's `>` test
+    }
+    // block maximum, then one atomic on the ordered bit pattern (s2 >= 0)
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, s2, o);
+        s2 = t > s2 ? t : s2;
+    }
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
+        if (m > 0.0) atomicMax(&scal->max_shift2_bits, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// Sweep A: DensityA (main.cpp:1665-1692), GravityCenter (1695-1727),
+// DensityP (1831-1858), DivergenceP (1860-1896), then
+// calculatePhysicalCoefficients (1631-1662) and the PressureP / PressureA
+// values (1904-1906, 1735-1740).
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(128)
+k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
+          const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
+          double* __restrict__ strain_p, double* __restrict__ div_p, double2* __restrict__ press,
+          double4* __restrict__ gcout, double* __restrict__ wall_center) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wall_center != nullptr && blockIdx.x == 0 && threadIdx.x < 12) {
+        // WallCenter += WallVelocity*Dt (main.cpp:2048-2052); the move kernel of
+        // this step has already used the old value.
+        const int t = threadIdx.x / 3, d = threadIdx.x % 3;
+        if (t >= 2) wall_center[3 * t + d] += c.wall_velocity[t][d] * c.dt;
+    }
+    if (i >= c.n) return;
+    const double4 pi = pos[i];
+    const double4 vi = vel[i];
+    const int ti = type_of(pi);
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    double sum_a = 0.0, sum_p = 0.0, sum_d = 0.0;
+    double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+        const int j = __ldg(nlist + (size_t)k * n + i);
+        if (j == i) continue;
+        const double4 pj = pos[j];
+        double x[3];
+        disp(c, pi, pj, x);
+        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        const bool in_a = c.ra2 - r2 >= 0;
+        const bool in_p = c.rp2 - r2 >= 0;
+        const bool in_g = ST && (c.rg2 - r2 >= 0);
+        if (!(in_a || in_p || in_g)) continue;
+        const double r = sqrt(r2);
+        double ratio = 1.0;
+        if (RATIO) ratio = c.ratio[ti][type_of(pj)];
+        if (in_a) {
+            const double w = RATIO ? ratio * f_wa(c, r) : f_wa(c, r);
+            sum_a += w;
+        }
+        if (ST && in_g) {
+            const double w = RATIO ? ratio * f_wg(c, r) : f_wg(c, r);
+            g0 += x[0] * w / c.r2g * c.rg;
+            g1 += x[1] * w / c.r2g * c.rg;
+            g2 += x[2] * w / c.r2g * c.rg;
+        }
+        if (in_p) {
+            sum_p += f_wp(c, r);
+            const double dw = f_dwpdr(c, r);
+            const double e0 = x[0] / r, e1 = x[1] / r, e2 = x[2] / r;
+            const double4 vj = vel[j];
+            const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+            sum_d -= u0 * e0 * dw;
+            sum_d -= u1 * e1 * dw;
+            sum_d -= u2 * e2 * dw;
+        }
+    }
+    dens_a[i] = sum_a;
+    const double strain = sum_p - c.n0p;
+    strain_p[i] = strain;
+    div_p[i] = sum_d;
+    if (ST) gcout[i] = make_double4(g0, g1, g2, 0.0);
+    double kappa = c.bulk_modulus[ti];
+    if (strain < 0.0) kappa = 0.0;
+    const double lambda = c.bulk_viscosity[ti];
+    const double pp = -lambda * sum_d + kappa * strain;
+    double pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
+    if (c.n0a <= sum_a) pa = 0.0;
+    press[i] = make_double2(pp, pa);
+}
+
+// Sweep B: PressureP force (main.cpp:1908-1938), PressureA force
+// (1742-1775), DiffuseInterface (1782-1828, aj uses the type of i as in the
+// reference), ViscosityV (1943-1984); Force = 0 + fP + fA + fDI + fV, then
+// Gravity (1988-1998) and Acceleration (2000-2010) for fluid particles.
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(128)
+k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
+          const double4* __restrict__ vel, double4* __restrict__ vel_out, const double2* __restrict__ press,
+          const double4* __restrict__ gc, const int* __restrict__ ncount, const int* __restrict__ nlist,
+          double4* __restrict__ force, StepScalars* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const double4 pi = pos[i];
+    const double4 vi = vel[i];
+    const double2 pri = press[i];
+    const int ti = type_of(pi);
+    const double mui = c.shear_viscosity[ti];
+    const double ai = c.a_k[ti];
+    double4 gci = make_double4(0, 0, 0, 0);
+    if (ST) gci = gc[i];
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;
+    double fa0 = 0.0, fa1 = 0.0, fa2 = 0.0;
+    double fd0 = 0.0, fd1 = 0.0, fd2 = 0.0;
+    double fv0 = 0.0, fv1 = 0.0, fv2 = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+        const int j = __ldg(nlist + (size_t)k * n + i);
+        if (j == i) continue;
+        const double4 pj = pos[j];
+        double x[3];
+        disp(c, pi, pj, x);
+        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        const bool in_p = c.rp2 - r2 > 0;
+        const bool in_a = c.ra2 - r2 > 0;
+        const bool in_g = ST && (c.rg2 - r2 > 0);
+        const bool in_v = c.rv2 - r2 > 0;
+        if (!(in_p || in_a || in_g || in_v)) continue;
+        const int tj = type_of(pj);
+        const double r = sqrt(r2);
+        const double e0 = x[0] / r, e1 = x[1] / r, e2 = x[2] / r;
+        double rij = 1.0, rji = 1.0;
+        if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
+        if (in_p) {
+            const double prj = press[j].x;
+            const double dw = f_dwpdr(c, r);
+            const double gw0 = dw * x[0] / r, gw1 = dw * x[1] / r, gw2 = dw * x[2] / r;
+            const double ps = pri.x + prj;
+            fp0 += ps * gw0 * c.vol;
+            fp1 += ps * gw1 * c.vol;
+            fp2 += ps * gw2 * c.vol;
+        }
+        if (in_a) {
+            const double paj = press[j].y;
+            const double dwa = f_dwadr(c, r);
+            const double dwij = RATIO ? rij * dwa : dwa;
+            const double dwji = RATIO ? rji * dwa : dwa;
+            const double s = pri.y * dwij + paj * dwji;
+            fa0 += s * e0 * c.vol;
+            fa1 += s * e1 * c.vol;
+            fa2 += s * e2 * c.vol;
+        }
+        if (ST && in_g) {
+            const double4 gcj = gc[j];
+            const double aj = ai;
+            const double wg = f_wg(c, r);
+            const double wij = RATIO ? rij * wg : wg;
+            const double wji = RATIO ? rji * wg : wg;
+            fd0 -= (aj * gcj.x * wji - ai * gci.x * wij) / c.r2g * c.rg * c.vol_over_l0;
+            fd1 -= (aj * gcj.y * wji - ai * gci.y * wij) / c.r2g * c.rg * c.vol_over_l0;
+            fd2 -= (aj * gcj.z * wji - ai * gci.z * wij) / c.r2g * c.rg * c.vol_over_l0;
+            const double dg = f_dwgdr(c, r);
+            const double dwij = RATIO ? rij * dg : dg;
+            const double dwji = RATIO ? rji * dg : dg;
+            double gr = 0.0;
+            gr += (aj * gcj.x * dwji - ai * gci.x * dwij) * x[0];
+            gr += (aj * gcj.y * dwji - ai * gci.y * dwij) * x[1];
+            gr += (aj * gcj.z * dwji - ai * gci.z * dwij) * x[2];
+            fd0 -= (gr) * e0 / c.r2g * c.rg * c.vol_over_l0;
+            fd1 -= (gr) * e1 / c.r2g * c.rg * c.vol_over_l0;
+            fd2 -= (gr) * e2 / c.r2g * c.rg * c.vol_over_l0;
+        }
+        if (in_v) {
+            const double dw = -f_dwvdr(c, r);
+            const double4 vj = vel[j];
+            const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+            const double muj = c.shear_viscosity[tj];
+            const double muij = 2.0 * (mui * muj) / (mui + muj);
+            const double dot = u0 * e0 + u1 * e1 + u2 * e2;
+            fv0 += c.visc_c * muij * dot * e0 * dw / r * c.vol;
+            fv1 += c.visc_c * muij * dot * e1 * dw / r * c.vol;
+            fv2 += c.visc_c * muij * dot * e2 * dw / r * c.vol;
+        }
+    }
+    double F0 = 0.0, F1 = 0.0, F2 = 0.0;   // resetForce (main.cpp:1617-1628)
+    F0 += fp0; F1 += fp1; F2 += fp2;
+    F0 += fa0; F1 += fa1; F2 += fa2;
+    F0 += fd0; F1 += fd1; F2 += fd2;
+    F0 += fv0; F1 += fv1; F2 += fv2;
+    double4 vn = vi;
+    const int nf = cellstart[c.tot];
+    if (i < nf) {
+        const double m = c.density[ti] * c.vol;
+        F0 += m * c.gravity[0];
+        F1 += m * c.gravity[1];
+        F2 += m * c.gravity[2];
+        vn.x += F0 / m * c.dt;
+        vn.y += F1 / m * c.dt;
+        vn.z += F2 / m * c.dt;
+        if (!(isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
+    }
+    force[i] = make_double4(F0, F1, F2, 0.0);
+    vel_out[i] = vn;
+}
+
+// Virial stress at particles, main.cpp:2057-2302: four sums (PressureP,
+// PressureA, ViscosityV, DiffuseInterface) added in that order.
+__global__ void __launch_bounds__(128)
+k_virial(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
+         const double2* __restrict__ press, const double4* __restrict__ gc, const int* __restrict__ ncount,
+         const int* __restrict__ nlist, double* __restrict__ virial_p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const double4 pi = pos[i];
+    const double4 vi = vel[i];
+    const int ti = type_of(pi);
+    const double2 pri = press[i];
+    const double4 gci = gc ? gc[i] : make_double4(0, 0, 0, 0);
+    const double mui = c.shear_viscosity[ti];
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    double S[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    for (int term = 0; term < 4; ++term) {
+        double st[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+        for (int k = 0; k < cnt; ++k) {
+            const int j = nlist[(size_t)k * n + i];
+            if (j == i) continue;
+            const double4 pj = pos[j];
+            double x[3];
+            disp(c, pi, pj, x);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            double f[3];
+            if (term == 0) {
+                if (!(c.rp2 - r2 > 0)) continue;
+                const double r = sqrt(r2);
+                const double dw = f_dwpdr(c, r);
+                const double g[3] = {dw * x[0] / r, dw * x[1] / r, dw * x[2] / r};
+                for (int d = 0; d < 3; ++d) f[d] = (pri.x) * g[d] * c.vol;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a][b] += 1.0 * f[a] * x[b] / c.vol;
+            } else if (term == 1) {
+                if (!(c.ra2 - r2 > 0)) continue;
+                const double ratio = c.ratio[ti][type_of(pj)];
+                const double r = sqrt(r2);
+                const double dw = ratio * f_dwadr(c, r);
+                const double g[3] = {dw * x[0] / r, dw * x[1] / r, dw * x[2] / r};
+                for (int d = 0; d < 3; ++d) f[d] = (pri.y) * g[d] * c.vol;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a][b] += 1.0 * f[a] * x[b] / c.vol;
+            } else if (term == 2) {
+                if (!(c.rv2 - r2 > 0)) continue;
+                const double r = sqrt(r2);
+                const double dw = -f_dwvdr(c, r);
+                const double e[3] = {x[0] / r, x[1] / r, x[2] / r};
+                const double4 vj = vel[j];
+                const double u[3] = {vj.x - vi.x, vj.y - vi.y, vj.z - vi.z};
+                const double muj = c.shear_viscosity[type_of(pj)];
+                const double muij = 2.0 * (mui * muj) / (mui + muj);
+                for (int d = 0; d < 3; ++d)
+                    f[d] = c.visc_c * muij * (u[0] * e[0] + u[1] * e[1] + u[2] * e[2]) * e[d] * dw / r * c.vol;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a][b] += 0.5 * f[a] * x[b] / c.vol;
+            } else {
+                if (!(c.rg2 - r2 > 0)) continue;
+                const double a_ = c.a_k[ti];
+                const double ratio = c.ratio[ti][type_of(pj)];
+                const double r = sqrt(r2);
+                const double w = ratio * f_wg(c, r);
+                const double gv[3] = {gci.x, gci.y, gci.z};
+                for (int d = 0; d < 3; ++d) f[d] = -a_ * (-gv[d]) * w / c.r2g * c.rg * c.vol_over_l0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a][b] += 1.0 * f[a] * x[b] / c.vol;
+                const double dw = ratio * f_dwgdr(c, r);
+                const double g[3] = {dw * x[0] / r, dw * x[1] / r, dw * x[2] / r};
+                double gr = 0.0;
+                for (int d = 0; d < 3; ++d) gr += (-gv[d]) * x[d];
+                for (int d = 0; d < 3; ++d) f[d] = -a_ * (gr) * g[d] / c.r2g * c.rg * c.vol_over_l0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) st[a][b] += 1.0 * f[a] * x[b] / c.vol;
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) S[a][b] += st[a][b];
+    }
+    if (c.dim == 2) virial_p[i] = -1.0 / 2.0 * (S[0][0] + S[1][1]);
+    else virial_p[i] = -1.0 / 3.0 * (S[0][0] + S[1][1] + S[2][2]);
+}
+
+// Fluid mass, momentum, kinetic energy: per-block partial sums in a fixed
+// order (deterministic), summed on the host.
+__global__ void __launch_bounds__(256)
+k_conserved(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
+            const double4* __restrict__ vel, double* __restrict__ partial) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s[5] = {0, 0, 0, 0, 0};
+    if (i < c.n && i < cellstart[c.tot]) {
+        const double m = c.density[type_of(pos[i])] * c.vol;
+        const double4 v = vel[i];
+        s[0] = m;
+        s[1] = m * v.x;
+        s[2] = m * v.y;
+        s[3] = m * v.z;
+        s[4] = 0.5 * m * (v.x * v.x + v.y * v.y + v.z * v.z);
+    }
+    __shared__ double sh[5][256];
+    for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] = s[k];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+            for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; ++k) partial[5 * (size_t)blockIdx.x + k] = sh[k][0];
+}
+
+inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel, const double4* snap,
+                 const double* wall_center, StepScalars* scal, cudaStream_t s) {
+    k_move<<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, snap, wall_center, scal);
+}
+
+void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,
+                    const int* ncount, const int* nlist, int cap_stride, double* dens_a, double* strain_p,
+                    double* div_p, double2* press, double4* gc, double* wall_center, cudaStream_t s) {
+    (void)cellstart;
+    (void)cap_stride;
+    const int nb = blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1;
+    if (c.has_st) {
+        if (c.ratio_all_one)
+            k_sweep_a<true, false><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+        else
+            k_sweep_a<true, true><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+    } else {
+        if (c.ratio_all_one)
+            k_sweep_a<false, false><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+        else
+            k_sweep_a<false, true><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+    }
+}
+
+void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
+                    double4* vel_out, const double2* press, const double4* gc, const int* ncount,
+                    const int* nlist, double4* force, StepScalars* scal, cudaStream_t s) {
+    const int nb = blocks(c.n, 128);
+    if (c.has_st) {
+        if (c.ratio_all_one)
+            k_sweep_b<true, false><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+        else
+            k_sweep_b<true, true><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+    } else {
+        if (c.ratio_all_one)
+            k_sweep_b<false, false><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+        else
+            k_sweep_b<false, true><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+    }
+}
+
+void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double2* press,
+                   const double4* gc, const int* ncount, const int* nlist, double* virial_p, cudaStream_t s) {
+    k_virial<<<blocks(c.n, 128), 128, 0, s>>>(c, pos, vel, press, gc, ncount, nlist, virial_p);
+}
+
+void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,
+                      double* partial, cudaStream_t s) {
+    k_conserved<<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, partial);
+}
+
+}  // namespace mph

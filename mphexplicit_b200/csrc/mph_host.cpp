@@ -1,0 +1,864 @@
+// mph_host.cpp — the C ABI (include/mph_b200.h): set-up constants, device
+// state, the per-step launch sequence, read-back and output.
+//
+// Step sequence of the FP64 form (the reference's loop body,
+// main.cpp:386-431):
+//   k_move        Convection + Wall + PeriodicBoundary + max displacement
+//   [rebuild]     cell index -> bitonic sort -> cell ranges -> reorder ->
+//                 neighbour list   (when the displacement test fires)
+//   k_sweep_a     DensityA, GravityCenter, DensityP, DivergenceP, coefficients,
+//                 PressureP/PressureA values
+//   k_sweep_b     all forces, gravity, acceleration
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "mph_internal.h"
+#include "mph_io.h"
+#include "mph_mixed.h"
+
+using mph::SimConst;
+using mph::StepScalars;
+
+// Per-kernel CUDA-event timing on the context stream (mph_profile_*).
+struct Profiler {
+    struct Pending {
+        int id;
+        int count;
+        cudaEvent_t a, b;
+    };
+    bool on = false;
+    std::vector<std::string> names;
+    std::vector<long long> launches;
+    std::vector<double> ms;
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+};
+
+struct mph_ctx {
+    int mode = MPH_MODE_FP64;
+    int dim = 3;
+    int n = 0;
+    mph_params p{};
+    mph_grid_header h{};
+    mph_constants c{};
+    SimConst sc{};
+    cudaStream_t stream = nullptr;
+    mph::DevFP64 d;
+    mph::MixedState* mixed = nullptr;
+    StepScalars* h_scal = nullptr;  // pinned
+    double time = 0.0;
+    long long step = 0, rebuilds = 0;
+    bool virial_valid = false;
+    int max_neighbors = 0;
+    long long launches = 0;
+    Profiler prof;
+    std::string err;
+};
+
+static thread_local std::string g_err;
+
+static cudaEvent_t take_event(mph_ctx* ctx) {
+    Profiler& p = ctx->prof;
+    if (!p.pool.empty()) {
+        cudaEvent_t e = p.pool.back();
+        p.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one launch (or one group of launches) of a named kernel: counts it
+// and, when profiling is on, records CUDA events around it on the ctx stream.
+struct Launch {
+    mph_ctx* ctx;
+    int id = -1;
+    int count = 1;
+    cudaEvent_t a = nullptr;
+    Launch(mph_ctx* c, const char* name) : ctx(c) {
+        Profiler& p = ctx->prof;
+        if (!p.on) return;
+        for (size_t k = 0; k < p.names.size(); ++k)
+            if (p.names[k] == name) id = (int)k;
+        if (id < 0) {
+            id = (int)p.names.size();
+            p.names.push_back(name);
+            p.launches.push_back(0);
+            p.ms.push_back(0.0);
+        }
+        a = take_event(ctx);
+        cudaEventRecord(a, ctx->stream);
+    }
+    ~Launch() {
+        ctx->launches += count;
+        if (id < 0) return;
+        cudaEvent_t b = take_event(ctx);
+        cudaEventRecord(b, ctx->stream);
+        ctx->prof.pending.push_back({id, count, a, b});
+    }
+};
+
+static int fail(mph_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, MPH_ERR_CUDA, std::string(#expr ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// set-up constants: initializeWeight (main.cpp:836-954), initializeFluid's
+// CofK/CofA (971-983), initializeWall (994-1033), initializeDomain (1035-1084).
+// Evaluated on the host in the reference's expression order.
+static double shape_wa(int dim, double swa, double r, double h) {
+    const double hp = dim == 2 ? h * h : h * h * h;
+    return 1.0 / swa * 1.0 / hp * (r / h) * (1.0 - (r / h)) * (1.0 - (r / h));
+}
+static double shape_wp(int dim, double swp, double r, double h) {
+    const double hp = dim == 2 ? h * h : h * h * h;
+    return 1.0 / swp * 1.0 / hp * ((1.0 - r / h) * (1.0 - r / h));
+}
+
+extern "C" int mph_compute_constants(const mph_params* p, const mph_grid_header* h, int dim, mph_constants* c) {
+    if (!p || !h || !c || (dim != 2 && dim != 3)) return fail(nullptr, MPH_ERR_ARG, "bad arguments");
+    if (!(h->particle_spacing > 0.0)) return fail(nullptr, MPH_ERR_ARG, "particle spacing must be > 0");
+    std::memset(c, 0, sizeof(*c));
+    const double l0 = h->particle_spacing;
+    c->dim = dim;
+    c->particle_volume = dim == 2 ? l0 * l0 : l0 * l0 * l0;
+    c->radius_a = p->radius_ratio_a * l0;
+    c->radius_g = p->radius_ratio_a * l0;  // RadiusRatioG = RadiusRatioA (main.cpp:838)
+    c->radius_p = p->radius_ratio_p * l0;
+    c->radius_v = p->radius_ratio_v * l0;
+    if (dim == 2) {
+        c->swa = 1.0 / 2.0 * 2.0 / 15.0 * M_PI / l0 / l0;
+        c->swg = 1.0 / 2.0 * 1.0 / 3.0 * M_PI / l0 / l0;
+        c->swp = 1.0 / 2.0 * 1.0 / 3.0 * M_PI / l0 / l0;
+        c->swv = 1.0 / 2.0 * 1.0 / 3.0 * M_PI / l0 / l0;
+        c->r2g = 1.0 / 2.0 * 1.0 / 30.0 * M_PI * c->radius_g * c->radius_g / l0 / l0 / c->swg;
+    } else {
+        c->swa = 1.0 / 3.0 * 1.0 / 5.0 * M_PI / l0 / l0 / l0;
+        c->swg = 1.0 / 3.0 * 2.0 / 5.0 * M_PI / l0 / l0 / l0;
+        c->swp = 1.0 / 3.0 * 2.0 / 5.0 * M_PI / l0 / l0 / l0;
+        c->swv = 1.0 / 3.0 * 2.0 / 5.0 * M_PI / l0 / l0 / l0;
+        c->r2g = 1.0 / 3.0 * 4.0 / 105.0 * M_PI * c->radius_g * c->radius_g / l0 / l0 / l0 / c->swg;
+    }
+    for (int which = 0; which < 2; ++which) {  // lattice sums N0a, N0p: origin excluded, r^2 <= R^2
+        const double R = which == 0 ? c->radius_a : c->radius_p;
+        const int range = (int)(R / l0 + 3.0);
+        const int zr = dim == 2 ? 0 : range;
+        double sum = 0.0;
+        int count = 0;
+        for (int ix = -range; ix <= range; ++ix)
+            for (int iy = -range; iy <= range; ++iy)
+                for (int iz = -zr; iz <= zr; ++iz) {
+                    if (ix == 0 && iy == 0 && iz == 0) continue;
+                    const double x = l0 * ((double)ix), y = l0 * ((double)iy), z = l0 * ((double)iz);
+                    const double r2 = dim == 2 ? x * x + y * y : x * x + y * y + z * z;
+                    if (r2 <= R * R) {
+                        const double r = std::sqrt(r2);
+                        sum += which == 0 ? shape_wa(dim, c->swa, r, R) : shape_wp(dim, c->swp, r, R);
+                        ++count;
+                    }
+                }
+        if (which == 0) { c->n0a = sum; c->n0a_count = count; }
+        else            { c->n0p = sum; c->n0p_count = count; }
+    }
+    double integN, integX;
+    if (dim == 2) { c->cof_k = 0.350778153; integN = 0.024679383; integX = 0.226126699; }
+    else          { c->cof_k = 0.326976006; integN = 0.021425779; integX = 0.233977488; }
+    for (int t = 0; t < MPH_TYPE_COUNT; ++t)
+        c->cof_a[t] = p->surface_tension[t] / ((c->radius_g / l0) * (integN + c->cof_k * c->cof_k * integX));
+    for (int t = 2; t < MPH_TYPE_COUNT; ++t) {  // theta = |omega|^2, no sqrt, as in the reference
+        const double* w = p->wall_omega[t];
+        double nrm[3] = {0.0, 0.0, 0.0}, q[4];
+        const double th = std::fabs(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        if (th != 0.0)
+            for (int d = 0; d < 3; ++d) nrm[d] = w[d] / th;
+        q[0] = nrm[0] * std::sin(th * p->dt / 2.0);
+        q[1] = nrm[1] * std::sin(th * p->dt / 2.0);
+        q[2] = nrm[2] * std::sin(th * p->dt / 2.0);
+        q[3] = std::cos(th * p->dt / 2.0);
+        double(*R)[3] = c->wall_rotation[t];
+        R[0][0] = q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3];
+        R[0][1] = 2.0 * (q[0] * q[1] - q[2] * q[3]);
+        R[0][2] = 2.0 * (q[0] * q[2] + q[1] * q[3]);
+        R[1][0] = 2.0 * (q[0] * q[1] + q[2] * q[3]);
+        R[1][1] = -q[0] * q[0] + q[1] * q[1] - q[2] * q[2] + q[3] * q[3];
+        R[1][2] = 2.0 * (q[1] * q[2] - q[0] * q[3]);
+        R[2][0] = 2.0 * (q[0] * q[2] - q[1] * q[3]);
+        R[2][1] = 2.0 * (q[1] * q[2] + q[0] * q[3]);
+        R[2][2] = -q[0] * q[0] - q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    }
+    double mr = 0.0;
+    mr = c->radius_a > mr ? c->radius_a : mr;
+    mr = c->radius_g > mr ? c->radius_g : mr;
+    mr = c->radius_p > mr ? c->radius_p : mr;
+    mr = c->radius_v > mr ? c->radius_v : mr;
+    c->max_radius = mr;
+    const double margin = 0.1 * l0;
+    double cc[3];
+    for (int d = 0; d < 3; ++d) c->domain_width[d] = h->domain_max[d] - h->domain_min[d];
+    cc[0] = std::floor((h->domain_max[0] - h->domain_min[0]) / (mr + margin));
+    cc[1] = std::floor((h->domain_max[1] - h->domain_min[1]) / (mr + margin));
+    cc[2] = dim == 2 ? 1 : std::floor((h->domain_max[2] - h->domain_min[2]) / (mr + margin));
+    for (int d = 0; d < 3; ++d) c->cell_count[d] = (int)cc[d];
+    c->total_cell_count = (int)(cc[0] * cc[1] * cc[2]);
+    for (int d = 0; d < 3; ++d) c->cell_width[d] = c->domain_width[d] / c->cell_count[d];
+    return MPH_OK;
+}
+
+// Kernel constants derived from mph_constants, in the reference's order.
+static int fill_simconst(mph_ctx* ctx) {
+    const mph_constants& c = ctx->c;
+    const mph_params& p = ctx->p;
+    SimConst& s = ctx->sc;
+    std::memset(&s, 0, sizeof(s));
+    const int dim = ctx->dim;
+    const double l0 = ctx->h.particle_spacing;
+    s.n = ctx->n;
+    s.dim = dim;
+    s.tot = c.total_cell_count;
+    for (int d = 0; d < 3; ++d) {
+        s.cc[d] = c.cell_count[d];
+        s.dmin[d] = ctx->h.domain_min[d];
+        s.width[d] = c.domain_width[d];
+        s.half_width[d] = 0.5 * c.domain_width[d];
+        s.cell_width[d] = c.cell_width[d];
+    }
+    if (s.cc[0] < 1 || s.cc[1] < 1 || s.cc[2] < 1 || s.tot < 1)
+        return fail(ctx, MPH_ERR_GEOMETRY, "domain narrower than one cell of MaxRadius+MARGIN");
+    if ((long long)s.cc[0] * s.cc[1] * s.cc[2] > (1LL << 29))
+        return fail(ctx, MPH_ERR_GEOMETRY, "too many cells");
+    const double rm = c.max_radius + 0.1 * l0;  // MaxRadius + MARGIN
+    s.rm2 = rm * rm;
+    s.range[0] = (int)std::ceil(rm / c.cell_width[0]);
+    s.range[1] = (int)std::ceil(rm / c.cell_width[1]);
+    s.range[2] = dim == 2 ? 0 : (int)std::ceil(rm / c.cell_width[2]);
+    for (int d = 0; d < 3; ++d)  // the reference asserts 2*range+1 <= 3 (main.cpp:1347-1349)
+        if (2 * s.range[d] + 1 > 3) return fail(ctx, MPH_ERR_GEOMETRY, "cell narrower than MaxRadius+MARGIN");
+    int pe = 0;
+    while ((ctx->n >> pe) != 0) ++pe;  // smallest power of two above n (main.cpp:612-617)
+    if (pe > 30) return fail(ctx, MPH_ERR_ARG, "too many particles");
+    s.pow2 = 1 << pe;
+    s.dt = p.dt;
+    s.l0 = l0;
+    s.vol = c.particle_volume;
+    s.vol_over_l0 = c.particle_volume / l0;
+    s.n0a = c.n0a;
+    s.n0p = c.n0p;
+    s.r2g = c.r2g;
+    s.cof_k = c.cof_k;
+    s.ra = c.radius_a; s.rg = c.radius_g; s.rp = c.radius_p; s.rv = c.radius_v;
+    s.ra2 = s.ra * s.ra; s.rg2 = s.rg * s.rg; s.rp2 = s.rp * s.rp; s.rv2 = s.rv * s.rv;
+    auto hp = [dim](double h) { return dim == 2 ? h * h : h * h * h; };
+    // 1.0/Sw * 1.0/h^D evaluated as ((1.0/Sw)*1.0)/h^D, main.cpp:215-284
+    s.ca = 1.0 / c.swa * 1.0 / hp(s.ra);
+    s.cg = 1.0 / c.swg * 1.0 / hp(s.rg);
+    s.cp = 1.0 / c.swp * 1.0 / hp(s.rp);
+    s.cv = 1.0 / c.swv * 1.0 / hp(s.rv);
+    s.inv_ra = 1.0 / s.ra; s.inv_rg = 1.0 / s.rg; s.inv_rp = 1.0 / s.rp; s.inv_rv = 1.0 / s.rv;
+    s.m2_rg = -2.0 / s.rg; s.m2_rp = -2.0 / s.rp; s.m2_rv = -2.0 / s.rv;
+    s.visc_c = dim == 2 ? 8.0 : 10.0;
+    const double margin = 0.1 * l0;
+    s.shift_thr = 0.5 * margin * 0.5 * margin;  // main.cpp:1102
+    s.has_st = 0;
+    s.ratio_all_one = 1;
+    for (int t = 0; t < MPH_TYPE_COUNT; ++t) {
+        s.density[t] = p.density[t];
+        s.bulk_modulus[t] = p.bulk_modulus[t];
+        s.bulk_viscosity[t] = p.bulk_viscosity[t];
+        s.shear_viscosity[t] = p.shear_viscosity[t];
+        s.cof_a[t] = c.cof_a[t];
+        s.a_k[t] = c.cof_a[t] * (c.cof_k) * (c.cof_k);
+        if (c.cof_a[t] != 0.0) s.has_st = 1;
+        for (int u = 0; u < MPH_TYPE_COUNT; ++u) {
+            s.ratio[t][u] = p.interaction_ratio[t][u];
+            if (p.interaction_ratio[t][u] != 1.0) s.ratio_all_one = 0;
+        }
+        for (int d = 0; d < 3; ++d) {
+            s.wall_velocity[t][d] = p.wall_velocity[t][d];
+            s.wall_omega[t][d] = p.wall_omega[t][d];
+            for (int e = 0; e < 3; ++e) s.wall_rot[t][d][e] = c.wall_rotation[t][d][e];
+        }
+    }
+    for (int d = 0; d < 3; ++d) s.gravity[d] = p.gravity[d];
+    return MPH_OK;
+}
+
+// ---------------------------------------------------------------------------
+template <class T>
+static int dalloc(mph_ctx* ctx, T** ptr, size_t count) {
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    const cudaError_t e = cudaMalloc((void**)ptr, count * sizeof(T));
+    if (e != cudaSuccess)
+        return fail(ctx, MPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return MPH_OK;
+}
+
+static void free_fp64(mph::DevFP64& d) {
+    void* ptrs[] = {d.pidx[0], d.pidx[1], d.type[0], d.type[1], d.pos[0], d.pos[1], d.vel[0], d.vel[1],
+                    d.snap, d.force, d.dens_a, d.strain_p, d.div_p, d.press, d.gc, d.virial_p, d.keys,
+                    d.vals, d.cellstart, d.ncount, d.nlist, d.wall_center, d.staging, d.scal};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    d = mph::DevFP64();
+}
+
+#define TRY(expr)                       \
+    do {                                \
+        const int st_ = (expr);         \
+        if (st_ != MPH_OK) return st_;  \
+    } while (0)
+
+static int alloc_fp64(mph_ctx* ctx) {
+    mph::DevFP64& d = ctx->d;
+    const size_t n = (size_t)ctx->n, P = (size_t)ctx->sc.pow2, tot = (size_t)ctx->sc.tot;
+    for (int k = 0; k < 2; ++k) {
+        TRY(dalloc(ctx, &d.pidx[k], n));
+        TRY(dalloc(ctx, &d.type[k], n));
+        TRY(dalloc(ctx, &d.pos[k], n));
+        TRY(dalloc(ctx, &d.vel[k], n));
+    }
+    TRY(dalloc(ctx, &d.snap, n));
+    TRY(dalloc(ctx, &d.force, n));
+    TRY(dalloc(ctx, &d.dens_a, n));
+    TRY(dalloc(ctx, &d.strain_p, n));
+    TRY(dalloc(ctx, &d.div_p, n));
+    TRY(dalloc(ctx, &d.press, n));
+    TRY(dalloc(ctx, &d.gc, n));
+    TRY(dalloc(ctx, &d.virial_p, n));
+    TRY(dalloc(ctx, &d.keys, P));
+    TRY(dalloc(ctx, &d.vals, P));
+    TRY(dalloc(ctx, &d.cellstart, 2 * tot + 1));
+    TRY(dalloc(ctx, &d.ncount, n));
+    TRY(dalloc(ctx, &d.wall_center, 12));
+    TRY(dalloc(ctx, &d.staging, 3 * n));
+    TRY(dalloc(ctx, &d.scal, 1));
+    CUDA_TRY(ctx, cudaMemsetAsync(d.gc, 0, n * sizeof(double4), ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(d.force, 0, n * sizeof(double4), ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(d.virial_p, 0, n * sizeof(double), ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(d.scal, 0, sizeof(StepScalars), ctx->stream));
+    return MPH_OK;
+}
+
+// Initial list length: lattice points within the cut-off, with head room for
+// compression; the build grows it when a longer list appears.
+static int initial_capacity(const mph_ctx* ctx) {
+    const double ratio = std::sqrt(ctx->sc.rm2) / ctx->h.particle_spacing;
+    const int r = (int)ratio + 1;
+    int cnt = 0;
+    const int zr = ctx->dim == 2 ? 0 : r;
+    for (int x = -r; x <= r; ++x)
+        for (int y = -r; y <= r; ++y)
+            for (int z = -zr; z <= zr; ++z)
+                if (x * x + y * y + z * z <= ratio * ratio) ++cnt;
+    int cap = (int)(cnt * 1.25) + 8;
+    cap = (cap + 31) / 32 * 32;
+    return cap;
+}
+
+static int grow_list(mph_ctx* ctx, int need) {
+    mph::DevFP64& d = ctx->d;
+    int cap = (int)(need * 1.15) + 8;
+    cap = (cap + 31) / 32 * 32;
+    if (d.nlist) cudaFree(d.nlist);
+    d.nlist = nullptr;
+    d.cap = 0;
+    TRY(dalloc(ctx, &d.nlist, (size_t)cap * (size_t)ctx->n));
+    d.cap = cap;
+    return MPH_OK;
+}
+
+// calculateCellParticle + calculateNeighbor (main.cpp:1111-1596).
+static int rebuild_fp64(mph_ctx* ctx) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    const int a = d.cur, b = 1 - d.cur, va = d.vcur, vb = 1 - d.vcur;
+    { Launch L(ctx, "cell_index"); mph::launch_cell_index(s, d.pos[a], d.type[a], d.keys, d.vals, st); }
+    { Launch L(ctx, "bitonic_sort"); L.count = mph::launch_bitonic_sort(s, d.keys, d.vals, st); }
+    { Launch L(ctx, "cell_ranges"); mph::launch_cell_ranges(s, d.keys, d.cellstart, st); }
+    {
+        Launch L(ctx, "reorder");
+        mph::launch_reorder(s, d.vals, d.pidx[a], d.type[a], d.pos[a], d.vel[va], d.pidx[b], d.type[b], d.pos[b],
+                            d.vel[vb], d.snap, st);
+    }
+    d.cur = b;
+    d.vcur = vb;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), st));
+        {
+            Launch L(ctx, "neighbor_list");
+            mph::launch_neighbor_list(s, d.pos[d.cur], d.keys, d.cellstart, d.ncount, d.nlist, d.cap, d.scal, st);
+        }
+        CUDA_TRY(ctx, cudaGetLastError());
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scal, d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        ctx->max_neighbors = ctx->h_scal->max_neighbors;
+        if (ctx->h_scal->max_neighbors <= d.cap) break;
+        TRY(grow_list(ctx, ctx->h_scal->max_neighbors));
+    }
+    if (ctx->max_neighbors > d.cap) return fail(ctx, MPH_ERR_CAPACITY, "neighbour table could not grow");
+    // the overflow flag of the attempts that grew the table is not an error
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->flags, 0, sizeof(int), st));
+    return MPH_OK;
+}
+
+static void sweep_a(mph_ctx* ctx, bool advance_wall) {
+    mph::DevFP64& d = ctx->d;
+    Launch L(ctx, "sweep_a");
+    mph::launch_sweep_a(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.ncount, d.nlist, d.cap, d.dens_a,
+                        d.strain_p, d.div_p, d.press, d.gc, advance_wall ? d.wall_center : nullptr, ctx->stream);
+}
+
+static int validate_inputs(int n, const int* type, const double* xyz, const double* vel) {
+    for (int i = 0; i < n; ++i) {
+        if (type[i] < 0 || type[i] >= MPH_TYPE_COUNT) return fail(nullptr, MPH_ERR_ARG, "particle type outside 0..3");
+        for (int d = 0; d < 3; ++d)
+            if (!std::isfinite(xyz[3 * (size_t)i + d]) || !std::isfinite(vel[3 * (size_t)i + d]))
+                return fail(nullptr, MPH_ERR_NONFINITE, "non-finite position or velocity in the input");
+    }
+    return MPH_OK;
+}
+
+extern "C" void mph_destroy(mph_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_fp64(ctx->d);
+    for (auto& q : ctx->prof.pending) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
+    for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
+    if (ctx->mixed) mph::mixed_destroy(ctx->mixed);
+    if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+static int create_impl(mph_ctx* ctx, const int* type, const double* xyz, const double* vel) {
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CUDA_TRY(ctx, cudaMallocHost((void**)&ctx->h_scal, sizeof(StepScalars)));
+    TRY(alloc_fp64(ctx));
+    mph::DevFP64& d = ctx->d;
+    const size_t n = (size_t)ctx->n;
+    cudaStream_t st = ctx->stream;
+    std::vector<int> pidx(n);
+    for (size_t i = 0; i < n; ++i) pidx[i] = (int)i;  // main.cpp:645-647
+    CUDA_TRY(ctx, cudaMemcpyAsync(d.pidx[0], pidx.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(d.type[0], type, n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    { Launch L(ctx, "unpack3"); mph::launch_unpack3(ctx->n, d.staging, d.pos[0], d.type[0], st); }
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    { Launch L(ctx, "unpack3"); mph::launch_unpack3(ctx->n, d.staging, d.vel[0], nullptr, st); }
+    double wc[12];
+    for (int t = 0; t < 4; ++t)
+        for (int k = 0; k < 3; ++k) wc[3 * t + k] = ctx->p.wall_center[t][k];
+    CUDA_TRY(ctx, cudaMemcpyAsync(d.wall_center, wc, sizeof(wc), cudaMemcpyHostToDevice, st));
+    d.cur = 0;
+    d.vcur = 0;
+    TRY(grow_list(ctx, initial_capacity(ctx)));
+    if (ctx->mode == MPH_MODE_MIXED) {
+        TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, st, &ctx->err));
+    }
+    // start-up: calculateCellParticle, calculateNeighbor, DensityA, GravityCenter,
+    // DensityP (main.cpp:358-364)
+    TRY(rebuild_fp64(ctx));
+    sweep_a(ctx, false);
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return MPH_OK;
+}
+
+extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim, int mode, const int* type,
+                          const double* xyz, const double* vel, mph_ctx** out) {
+    if (!out) return fail(nullptr, MPH_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!p || !h || !type || !xyz || !vel) return fail(nullptr, MPH_ERR_ARG, "NULL argument");
+    if (dim != 2 && dim != 3) return fail(nullptr, MPH_ERR_ARG, "dim must be 2 or 3");
+    if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED) return fail(nullptr, MPH_ERR_ARG, "unknown mode");
+    if (h->particle_count <= 0) return fail(nullptr, MPH_ERR_ARG, "particle_count must be > 0");
+    if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, MPH_ERR_ARG, "Dt must be finite and > 0");
+    for (int d = 0; d < 3; ++d)
+        if (!(h->domain_max[d] > h->domain_min[d])) return fail(nullptr, MPH_ERR_ARG, "empty domain");
+    TRY(validate_inputs(h->particle_count, type, xyz, vel));
+    mph_ctx* ctx = new mph_ctx();
+    ctx->mode = mode;
+    ctx->dim = dim;
+    ctx->n = h->particle_count;
+    ctx->p = *p;
+    ctx->h = *h;
+    ctx->time = h->time;
+    int st = mph_compute_constants(p, h, dim, &ctx->c);
+    if (st == MPH_OK) st = fill_simconst(ctx);
+    if (st == MPH_OK) st = create_impl(ctx, type, xyz, vel);
+    if (st != MPH_OK) {
+        g_err = ctx->err.empty() ? g_err : ctx->err;
+        mph_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return MPH_OK;
+}
+
+static int read_scalars(mph_ctx* ctx) {
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scal, ctx->d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return MPH_OK;
+}
+
+static int check_flags(mph_ctx* ctx) {
+    const int f = ctx->h_scal->flags;
+    if (f & mph::DEVFLAG_NONFINITE) return fail(ctx, MPH_ERR_NONFINITE, "non-finite velocity produced by a step");
+    if (f & mph::DEVFLAG_NEIGHBOR_OVERFLOW) return fail(ctx, MPH_ERR_CAPACITY, "neighbour table overflow");
+    if (f) return fail(ctx, MPH_ERR_DEVICE, "device error flag " + std::to_string(f));
+    return MPH_OK;
+}
+
+static int step_fp64(mph_ctx* ctx, int nsteps) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    for (int k = 0; k < nsteps; ++k) {
+        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+        {
+            Launch L(ctx, "move");
+            mph::launch_move(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap, d.wall_center, d.scal, st);
+        }
+        TRY(read_scalars(ctx));
+        TRY(check_flags(ctx));
+        double ms;
+        std::memcpy(&ms, &ctx->h_scal->max_shift2_bits, sizeof(double));
+        if (ms > s.shift_thr) {  // neighborCalculation() == 1 (main.cpp:1102)
+            TRY(rebuild_fp64(ctx));
+            ++ctx->rebuilds;
+        }
+        sweep_a(ctx, true);
+        {
+            Launch L(ctx, "sweep_b");
+            mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.vel[1 - d.vcur], d.press, d.gc,
+                                d.ncount, d.nlist, d.force, d.scal, st);
+        }
+        d.vcur = 1 - d.vcur;
+        CUDA_TRY(ctx, cudaGetLastError());
+        ctx->time += ctx->p.dt;  // main.cpp:449
+        ++ctx->step;
+    }
+    ctx->virial_valid = false;
+    return MPH_OK;
+}
+
+extern "C" int mph_step(mph_ctx* ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    if (ctx->mode == MPH_MODE_MIXED) {
+        const int st = mph::mixed_step(ctx->mixed, ctx->sc, ctx->d, nsteps, ctx->stream, &ctx->err);
+        if (st != MPH_OK) return st;
+        ctx->time += ctx->p.dt * nsteps;  // Time += Dt per step (main.cpp:449)
+        ctx->step += nsteps;
+        ctx->virial_valid = false;
+        return MPH_OK;
+    }
+    return step_fp64(ctx, nsteps);
+}
+
+extern "C" int mph_synchronize(mph_ctx* ctx) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    TRY(read_scalars(ctx));
+    return check_flags(ctx);
+}
+
+// The mixed form keeps its own particle order between rebuilds; bring the
+// FP64 buffers up to date before any read-back.
+static int sync_state(mph_ctx* ctx) {
+    if (ctx->mode == MPH_MODE_MIXED) TRY(mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err));
+    return MPH_OK;
+}
+
+extern "C" int mph_get_info(mph_ctx* ctx, mph_info* info) {
+    if (!ctx || !info) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    TRY(sync_state(ctx));
+    std::memset(info, 0, sizeof(*info));
+    info->particle_count = ctx->n;
+    int cs[3] = {0, 0, 0};
+    const int tot = ctx->sc.tot;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&cs[0], ctx->d.cellstart, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&cs[1], ctx->d.cellstart + tot, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(&cs[2], ctx->d.cellstart + 2 * tot, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<int> nc(ctx->n);
+    if (ctx->mode == MPH_MODE_FP64)
+        CUDA_TRY(ctx, cudaMemcpyAsync(nc.data(), ctx->d.ncount, nc.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    long long total = 0;
+    for (int v : nc) total += v;
+    info->fluid_particle_begin = cs[0];
+    info->fluid_particle_end = cs[1];
+    info->wall_particle_begin = cs[1];
+    info->wall_particle_end = cs[2];
+    info->neighbor_ind_count = total;
+    info->max_neighbor_count = ctx->max_neighbors;
+    info->neighbor_capacity = ctx->d.cap;
+    info->step = ctx->step;
+    info->rebuild_count = ctx->mode == MPH_MODE_MIXED ? mph::mixed_rebuilds(ctx->mixed) : ctx->rebuilds;
+    info->time = ctx->time;
+    info->mode = ctx->mode;
+    return MPH_OK;
+}
+
+extern "C" int mph_get_constants(mph_ctx* ctx, mph_constants* c) {
+    if (!ctx || !c) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    *c = ctx->c;
+    return MPH_OK;
+}
+
+static int d2h_vec3(mph_ctx* ctx, const double4* src, double* dst) {
+    { Launch L(ctx, "pack3"); mph::launch_pack3(ctx->n, src, ctx->d.staging, ctx->stream); }
+    CUDA_TRY(ctx, cudaMemcpyAsync(dst, ctx->d.staging, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return MPH_OK;
+}
+
+template <class T>
+static int d2h(mph_ctx* ctx, T* dst, const T* src, size_t count) {
+    if (!dst) return MPH_OK;
+    CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    return MPH_OK;
+}
+
+extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, double* xyz, double* vel, double* force,
+                             int* neighbor_count, double* density_a, double* vol_strain_p, double* virial_pressure) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    TRY(sync_state(ctx));
+    mph::DevFP64& d = ctx->d;
+    const size_t n = (size_t)ctx->n;
+    TRY(d2h(ctx, particle_index, d.pidx[d.cur], n));
+    TRY(d2h(ctx, type, d.type[d.cur], n));
+    TRY(d2h(ctx, neighbor_count, d.ncount, n));
+    TRY(d2h(ctx, density_a, d.dens_a, n));
+    TRY(d2h(ctx, vol_strain_p, d.strain_p, n));
+    TRY(d2h(ctx, virial_pressure, d.virial_p, n));
+    if (xyz) TRY(d2h_vec3(ctx, d.pos[d.cur], xyz));
+    if (vel) TRY(d2h_vec3(ctx, d.vel[d.vcur], vel));
+    if (force) TRY(d2h_vec3(ctx, d.force, force));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return MPH_OK;
+}
+
+extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    TRY(sync_state(ctx));
+    mph::DevFP64& d = ctx->d;
+    const size_t n = (size_t)ctx->n;
+    cudaStream_t st = ctx->stream;
+    if (xyz) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+        Launch L(ctx, "unpack3");
+        mph::launch_unpack3(ctx->n, d.staging, d.pos[d.cur], d.type[d.cur], st);
+    }
+    if (vel) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+        Launch L(ctx, "unpack3");
+        mph::launch_unpack3(ctx->n, d.staging, d.vel[d.vcur], nullptr, st);
+    }
+    if (ctx->mode == MPH_MODE_MIXED) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
+    CUDA_TRY(ctx, cudaGetLastError());
+    return MPH_OK;
+}
+
+extern "C" int mph_get_fields(mph_ctx* ctx, double* divergence_p, double* pressure_p, double* pressure_a,
+                              double* gravity_center) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    TRY(sync_state(ctx));
+    mph::DevFP64& d = ctx->d;
+    const size_t n = (size_t)ctx->n;
+    TRY(d2h(ctx, divergence_p, d.div_p, n));
+    if (pressure_p || pressure_a) {
+        std::vector<double2> pr(n);
+        CUDA_TRY(ctx, cudaMemcpyAsync(pr.data(), d.press, n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        for (size_t i = 0; i < n; ++i) {
+            if (pressure_p) pressure_p[i] = pr[i].x;
+            if (pressure_a) pressure_a[i] = pr[i].y;
+        }
+    }
+    if (gravity_center) TRY(d2h_vec3(ctx, d.gc, gravity_center));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return MPH_OK;
+}
+
+extern "C" int mph_get_cells(mph_ctx* ctx, int* cell_index, int* fb, int* fe, int* wb, int* we) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "cell data is kept by the FP64 form only");
+    const int tot = ctx->sc.tot;
+    std::vector<int> cs(2 * (size_t)tot + 1);
+    TRY(d2h(ctx, cell_index, ctx->d.keys, (size_t)ctx->n));
+    CUDA_TRY(ctx, cudaMemcpyAsync(cs.data(), ctx->d.cellstart, cs.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < tot; ++c) {
+        if (fb) fb[c] = cs[c];
+        if (fe) fe[c] = cs[c + 1];
+        if (wb) wb[c] = cs[c + tot];
+        if (we) we[c] = cs[c + tot + 1];
+    }
+    return MPH_OK;
+}
+
+extern "C" int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long long ind_capacity) {
+    if (!ctx || !ptr) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "the neighbour list is kept by the FP64 form only");
+    const size_t n = (size_t)ctx->n;
+    std::vector<int> nc(n);
+    CUDA_TRY(ctx, cudaMemcpyAsync(nc.data(), ctx->d.ncount, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ptr[0] = 0;
+    for (size_t i = 0; i < n; ++i) ptr[i + 1] = ptr[i] + nc[i];
+    if (!ind) return MPH_OK;
+    if (ptr[n] > ind_capacity) return fail(ctx, MPH_ERR_ARG, "ind_capacity too small");
+    const int cap = ctx->d.cap;
+    std::vector<int> tab((size_t)cap * n);
+    CUDA_TRY(ctx, cudaMemcpyAsync(tab.data(), ctx->d.nlist, tab.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < nc[i]; ++k) ind[ptr[i] + k] = tab[(size_t)k * n + i];
+    return MPH_OK;
+}
+
+extern "C" int mph_compute_virial(mph_ctx* ctx) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "virial stress is computed by the FP64 form");
+    mph::DevFP64& d = ctx->d;
+    {
+        Launch L(ctx, "virial");
+        mph::launch_virial(ctx->sc, d.pos[d.cur], d.vel[d.vcur], d.press, d.gc, d.ncount, d.nlist, d.virial_p,
+                           ctx->stream);
+    }
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->virial_valid = true;
+    return MPH_OK;
+}
+
+extern "C" int mph_write_vtk(mph_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    const size_t n = (size_t)ctx->n;
+    std::vector<int> type(n), nc(n);
+    std::vector<double> x(3 * n), v(3 * n), f(3 * n), da(n), sp(n), vp(n);
+    TRY(mph_get_state(ctx, nullptr, type.data(), x.data(), v.data(), f.data(), nc.data(), da.data(), sp.data(),
+                      vp.data()));
+    const int st = mph::write_vtk_host(path, ctx->n, type.data(), x.data(), v.data(), f.data(), nc.data(), da.data(),
+                                       sp.data(), vp.data());
+    if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
+    return MPH_OK;
+}
+
+extern "C" int mph_write_vtk_arrays(const char* path, int n, const int* type, const double* xyz, const double* vel,
+                                    const double* force, const int* neighbor_count, const double* density_a,
+                                    const double* vol_strain_p, const double* virial_pressure) {
+    if (!path || n < 0 || (n > 0 && (!type || !xyz || !vel || !force || !neighbor_count || !density_a ||
+                                     !vol_strain_p || !virial_pressure)))
+        return fail(nullptr, MPH_ERR_ARG, "bad arguments");
+    const int st = mph::write_vtk_host(path, n, type, xyz, vel, force, neighbor_count, density_a, vol_strain_p,
+                                       virial_pressure);
+    if (st != MPH_OK) return fail(nullptr, st, std::string("cannot write ") + path);
+    return MPH_OK;
+}
+
+extern "C" int mph_write_prof(mph_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    const size_t n = (size_t)ctx->n;
+    std::vector<int> type(n);
+    std::vector<double> x(3 * n), v(3 * n);
+    TRY(mph_get_state(ctx, nullptr, type.data(), x.data(), v.data(), nullptr, nullptr, nullptr, nullptr, nullptr));
+    mph_grid_header h = ctx->h;
+    h.time = ctx->time;
+    const int st = mph_write_grid_file(path, &h, type.data(), x.data(), v.data());
+    if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
+    return MPH_OK;
+}
+
+extern "C" int mph_conserved_sums(mph_ctx* ctx, double out[5]) {
+    if (!ctx || !out) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    TRY(sync_state(ctx));
+    mph::DevFP64& d = ctx->d;
+    const int nb = (ctx->n + 255) / 256;
+    double* part = nullptr;
+    TRY(dalloc(ctx, &part, 5 * (size_t)nb));
+    { Launch L(ctx, "conserved"); mph::launch_conserved(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], part, ctx->stream); }
+    std::vector<double> h(5 * (size_t)nb);
+    cudaError_t e = cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(part);
+    if (e != cudaSuccess) return fail(ctx, MPH_ERR_CUDA, cudaGetErrorString(e));
+    for (int k = 0; k < 5; ++k) out[k] = 0.0;
+    for (int b = 0; b < nb; ++b)
+        for (int k = 0; k < 5; ++k) out[k] += h[5 * (size_t)b + k];
+    return MPH_OK;
+}
+
+extern "C" void* mph_stream(mph_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+extern "C" long long mph_launch_count(mph_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+static int profile_collect(mph_ctx* ctx) {
+    Profiler& p = ctx->prof;
+    if (p.pending.empty()) return MPH_OK;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (const auto& q : p.pending) {
+        float ms = 0.0f;
+        CUDA_TRY(ctx, cudaEventElapsedTime(&ms, q.a, q.b));
+        p.ms[q.id] += ms;
+        p.launches[q.id] += q.count;
+        p.pool.push_back(q.a);
+        p.pool.push_back(q.b);
+    }
+    p.pending.clear();
+    return MPH_OK;
+}
+
+extern "C" int mph_profile_enable(mph_ctx* ctx, int enable) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    TRY(profile_collect(ctx));
+    Profiler& p = ctx->prof;
+    p.on = enable != 0;
+    if (p.on) {
+        p.names.clear();
+        p.launches.clear();
+        p.ms.clear();
+    }
+    return MPH_OK;
+}
+
+extern "C" int mph_profile_read(mph_ctx* ctx, mph_kernel_stat* out, int capacity, int* count) {
+    if (!ctx || !count || (capacity > 0 && !out)) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    TRY(profile_collect(ctx));
+    const Profiler& p = ctx->prof;
+    *count = (int)p.names.size();
+    for (int k = 0; k < (int)p.names.size() && k < capacity; ++k) {
+        std::snprintf(out[k].name, sizeof(out[k].name), "%s", p.names[k].c_str());
+        out[k].launches = p.launches[k];
+        out[k].total_ms = p.ms[k];
+    }
+    return MPH_OK;
+}
+
+extern "C" int mph_last_error(mph_ctx* ctx, char* buf, int len) {
+    if (!buf || len <= 0) return MPH_ERR_ARG;
+    const std::string& m = ctx ? ctx->err : g_err;
+    std::snprintf(buf, (size_t)len, "%s", m.c_str());
+    return MPH_OK;
+}
+
+extern "C" const char* mph_version(void) { return "mph_b200 0.1 (sm_100a)"; }

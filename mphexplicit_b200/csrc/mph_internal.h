@@ -1,0 +1,121 @@
+// mph_internal.h — device constants, context layout and kernel launchers of the
+// B200 MPH-WC explicit step.  Shared by the host orchestration (mph_host.cpp)
+// and the CUDA translation units (k_cells.cu, k_fp64.cu, k_mixed.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include "mph_b200.h"
+
+namespace mph {
+
+// Everything a step kernel needs that is fixed between rebuilds, passed by
+// value (kernel parameter space) so no constant-memory upload is needed.
+// The kernel-shape prefactors are evaluated on the host in the reference's
+// operation order (main.cpp:214-284): e.g. wa = ((ca*q)*(1-q))*(1-q) with
+// ca = (1/Swa)/h^D and q = r/h.
+struct SimConst {
+    int n;                 // particle count
+    int dim;
+    int tot;               // TotalCellCount
+    int cc[3];             // CellCount
+    int range[3];          // stencil half-width per axis (1, or 0 for z in 2-D)
+    int pow2;              // PowerParticleCount
+    int has_st;            // any surface tension -> diffuse-interface terms
+    int ratio_all_one;     // InteractionRatio == 1 everywhere
+    double dmin[3], width[3], half_width[3], cell_width[3];
+    double dt, l0, vol, vol_over_l0;
+    double n0a, n0p, r2g, cof_k;
+    double ra, rg, rp, rv;             // radii
+    double ra2, rg2, rp2, rv2;         // radius*radius
+    double rm2;                        // (MaxRadius+MARGIN)^2, neighbour cut-off
+    double ca, cg, cp, cv;             // (1/Sw)/h^D for wa, wg/dwg, wp/dwp, dwv
+    double inv_ra, inv_rg, inv_rp, inv_rv;  // 1.0/h
+    double m2_rg, m2_rp, m2_rv;        // -2.0/h
+    double visc_c;                     // 8 (2-D) or 10 (3-D)
+    double shift_thr;                  // 0.5*MARGIN*0.5*MARGIN
+    double density[MPH_TYPE_COUNT], bulk_modulus[MPH_TYPE_COUNT];
+    double bulk_viscosity[MPH_TYPE_COUNT], shear_viscosity[MPH_TYPE_COUNT];
+    double cof_a[MPH_TYPE_COUNT], a_k[MPH_TYPE_COUNT];  // a_k = CofA*CofK*CofK
+    double ratio[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
+    double gravity[3];
+    double wall_velocity[MPH_TYPE_COUNT][3], wall_omega[MPH_TYPE_COUNT][3];
+    double wall_rot[MPH_TYPE_COUNT][3][3];
+};
+
+// Small per-step device scalars (one cache line, read back with one copy).
+struct StepScalars {
+    unsigned long long max_shift2_bits;  // max |shift|^2 as ordered bits (>= 0)
+    int flags;                           // MPH_DEVFLAG_*
+    int max_neighbors;                   // longest list of the last build
+    int rebuild;                         // decision of the last move kernel
+    int pad[11];
+};
+
+enum : int {
+    DEVFLAG_NEIGHBOR_OVERFLOW = 1,
+    DEVFLAG_NONFINITE = 2,
+    DEVFLAG_CELL_RANGE = 4,
+};
+
+// Device buffers of the FP64 form.  Arrays are in cell-sorted order.
+struct DevFP64 {
+    int* pidx[2] = {nullptr, nullptr};
+    int* type[2] = {nullptr, nullptr};
+    double4* pos[2] = {nullptr, nullptr};   // x,y,z,(double)type
+    double4* vel[2] = {nullptr, nullptr};   // vx,vy,vz,0
+    int cur = 0;                            // index of the current pos/type/pidx
+    int vcur = 0;                           // index of the current velocity
+    double4* snap = nullptr;                // NeighborCalculatedPosition
+    double4* force = nullptr;
+    double* dens_a = nullptr;
+    double* strain_p = nullptr;
+    double* div_p = nullptr;
+    double2* press = nullptr;               // {PressureP, PressureA}
+    double4* gc = nullptr;                  // GravityCenter
+    double* virial_p = nullptr;
+    int* keys = nullptr;                    // CellIndex (sorted), pow2 entries
+    int* vals = nullptr;                    // CellParticle, pow2 entries
+    int* cellstart = nullptr;               // 2*tot+1: #keys below each key value
+    int* ncount = nullptr;                  // NeighborCount
+    int* nlist = nullptr;                   // [cap][n] column-major list
+    int cap = 0;
+    double* wall_center = nullptr;          // [4][3], advanced on the device
+    double* staging = nullptr;              // [n][3] pack/unpack buffer
+    StepScalars* scal = nullptr;
+};
+
+// ---- kernel launchers (k_cells.cu) ----------------------------------------
+void launch_cell_index(const SimConst& c, const double4* pos, const int* type, int* keys,
+                       int* vals, cudaStream_t s);
+int launch_bitonic_sort(const SimConst& c, int* keys, int* vals, cudaStream_t s);  // returns #launches
+void launch_cell_ranges(const SimConst& c, const int* keys, int* cellstart, cudaStream_t s);
+void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, const int* type_in,
+                    const double4* pos_in, const double4* vel_in, int* pidx_out, int* type_out,
+                    double4* pos_out, double4* vel_out, double4* snap, cudaStream_t s);
+void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys,
+                          const int* cellstart, int* ncount, int* nlist, int cap,
+                          StepScalars* scal, cudaStream_t s);
+void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);
+void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s);
+
+// ---- kernel launchers (k_fp64.cu) -----------------------------------------
+void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel,
+                 const double4* snap, const double* wall_center, StepScalars* scal,
+                 cudaStream_t s);
+void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
+                    const double4* vel, const int* ncount, const int* nlist, int cap_stride,
+                    double* dens_a, double* strain_p, double* div_p, double2* press, double4* gc,
+                    double* wall_center, cudaStream_t s);
+void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
+                    const double4* vel_in, double4* vel_out, const double2* press,
+                    const double4* gc, const int* ncount, const int* nlist, double4* force,
+                    StepScalars* scal, cudaStream_t s);
+void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double2* press,
+                   const double4* gc, const int* ncount, const int* nlist, double* virial_p,
+                   cudaStream_t s);
+void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos,
+                      const double4* vel, double* out5, cudaStream_t s);
+
+}  // namespace mph

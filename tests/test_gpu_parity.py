@@ -1,0 +1,179 @@
+"""CUDA FP64 form vs the reference, through the C ABI (needs a B200).
+
+The FP64 form keeps the reference's operation order, its bitonic cell sort and
+its neighbour-list order, so every comparison here is bit-exact:
+  * golden fixtures: the reference's own arrays after k steps;
+  * fresh seeded scenes: the CPU oracle (itself pinned to the reference);
+  * output files: byte-identical *.vtk / *.prof text;
+  * full-size benchmark scene (2.78 M particles): two steps against the oracle.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import mphexplicit_b200 as M
+from mphexplicit_b200 import _native as N
+from mphexplicit_b200 import scenes
+from oracle import pyoracle as po
+from tests.common import CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+def solver_for(case: GoldenCase, mode="fp64") -> M.Solver:
+    return M.Solver.from_files(case.data, case.grid, dim=case.dim, mode=mode)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_matches_reference_golden(name):
+    case = GoldenCase(name)
+    s = solver_for(case)
+    s.step(case.steps)
+    s.synchronize()
+    s.compute_virial()
+    st, f, c = s.state(), s.fields(), s.cells()
+    for k in STATE_KEYS:
+        assert_same(st[k], case.ref[k], k)
+    for k in FIELD_KEYS:
+        if k == "gravity_center" and not any(s.params.surface_tension[t] for t in range(4)):
+            continue  # not computed without surface tension (every term is zero then)
+        assert_same(f[k], case.ref[k], k)
+    for k in CELL_KEYS:
+        assert_same(c[k], case.ref[k], k)
+    ptr, ind = s.neighbors()
+    assert_same(ptr, case.ref["nptr"], "NeighborPtr")
+    assert_same(ind, case.ref["nind"], "NeighborInd")
+    info = s.info()
+    assert info["rebuild_count"] == case.rebuilds
+    assert info["neighbor_ind_count"] == case.neighbor_ind_count
+    assert info["time"] == float(case.ref["time"])
+    s.close()
+
+
+def test_startup_matches_oracle():
+    case = GoldenCase("bridge")
+    p = M.read_data_file(case.data)
+    g = M.read_grid_file(case.grid)
+    o = po.Oracle(p, g.header, g.type, g.xyz, g.vel, 2)
+    s = M.Solver(p, g.header, g.type, g.xyz, g.vel, dim=2)
+    a, b = s.state(), o.state()
+    for k in ["particle_index", "type", "xyz", "vel", "neighbor_count", "density_a", "vol_strain_p"]:
+        assert_same(a[k], b[k], k)
+    for k in CELL_KEYS:
+        assert_same(s.cells()[k], o.cells()[k], k)
+    assert_same(s.fields()["gravity_center"], o.fields()["gravity_center"], "gc")
+
+
+def _fresh():
+    yield scenes.droplet_2d(n=24, seed=21, steps=60), 60, {}
+    yield scenes.dam_break_3d(fluid=(16, 12, 24), box=(40, 12, 30), walls=3, seed=22), 30, {}
+    sc = scenes.two_fluid_column(n=14, seed=23, steps=40)
+    yield sc, 25, {"ratio": True}
+    sc = scenes.dam_break_3d(fluid=(10, 6, 10), box=(24, 6, 16), walls=2, seed=24)
+    sc.params.wall_omega[2][1] = 0.4
+    sc.params.wall_velocity[2][0] = 0.03
+    sc.params.wall_center[2][2] = 0.02
+    yield sc, 30, {}
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_fp64_matches_oracle_fresh(k):
+    sc, steps, opt = list(_fresh())[k]
+    if opt.get("ratio"):
+        rng = np.random.default_rng(k)
+        for a in range(4):
+            for b in range(4):
+                sc.params.interaction_ratio[a][b] = float(rng.uniform(0.6, 1.4))
+    o = po.Oracle.from_scene(sc)
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim)
+    o.step(steps)
+    s.step(steps)
+    o.virial()
+    s.compute_virial()
+    a, b = s.state(), o.state()
+    for key in STATE_KEYS:
+        assert_same(a[key], b[key], f"{sc.name}:{key}")
+    assert s.info()["rebuild_count"] == o.rebuilds
+
+
+@pytest.mark.parametrize("name", ["square_drop_skip", "dam_break_small"])
+def test_output_files_match_reference_bytes(name):
+    case = GoldenCase(name)
+    s = solver_for(case)
+    s.step(case.steps)
+    s.compute_virial()
+    with tempfile.TemporaryDirectory() as td:
+        vtk, prof = os.path.join(td, "a.vtk"), os.path.join(td, "a.prof")
+        s.write_vtk(vtk)
+        s.write_prof(prof)
+        assert open(vtk, "rb").read() == case.reference_bytes("vtk")
+        assert open(prof, "rb").read() == case.reference_bytes("prof")
+
+
+def test_state_round_trip_and_step_continuity():
+    """get_state -> set_state leaves the trajectory unchanged (host-resident use)."""
+    sc = scenes.dam_break_3d(fluid=(8, 8, 12), box=(20, 8, 16), seed=5)
+    a = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3)
+    b = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3)
+    x = np.zeros((sc.n, 3))
+    v = np.zeros((sc.n, 3))
+    for _ in range(20):
+        a.step(1)
+        a.get_xv(x, v)
+        a.set_state(x, v)
+        b.step(1)
+    for key in STATE_KEYS:
+        assert_same(a.state()[key], b.state()[key], key)
+
+
+def test_nonfinite_state_is_reported_not_trapped():
+    """A NaN velocity injected from the host is caught by the device-side
+    finiteness flag and returned as MPH_ERR_NONFINITE; the context stays usable."""
+    sc = scenes.droplet_2d(n=12, seed=3)
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
+    st = s.state()
+    v = st["vel"].copy()
+    v[5, 0] = np.nan
+    s.set_state(st["xyz"], v)
+    with pytest.raises(M.MphError) as e:
+        s.step(2)
+        s.synchronize()
+    assert e.value.code == N.MPH_ERR_NONFINITE
+    s.close()
+    t = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)  # device still fine
+    t.step(3)
+    t.synchronize()
+
+
+def test_neighbor_table_grows_on_compression():
+    """Squeezing particles closer than the lattice spacing makes lists longer
+    than the initial table; the build grows it and stays exact."""
+    sc = scenes.droplet_2d(n=20, seed=9)
+    c = sc.xyz.mean(axis=0)
+    sc.xyz[:] = c + (sc.xyz - c) * 0.6
+    o = po.Oracle.from_scene(sc)
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
+    assert s.info()["max_neighbor_count"] > 100
+    assert_same(s.state()["neighbor_count"], o.state()["neighbor_count"], "ncount")
+    p1, i1 = s.neighbors()
+    p2, i2 = o.neighbors()
+    assert_same(i1, i2, "nind")
+
+
+def test_full_size_dam_break_two_steps():
+    """Benchmark config 2 at full size (2.0 M fluid + 0.78 M wall): two steps,
+    bit-exact against the oracle, and the expected interior neighbour count."""
+    sc = scenes.dam_break_3d()
+    assert sc.n == 2_779_256
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3)
+    s.step(2)
+    a = s.state()
+    o = po.Oracle.from_scene(sc)
+    o.step(2)
+    b = o.state()
+    for key in ["particle_index", "type", "xyz", "vel", "neighbor_count", "density_a", "vol_strain_p", "force"]:
+        assert_same(a[key], b[key], key)
+    fluid = a["type"] < 2
+    assert np.median(a["neighbor_count"][fluid]) >= 180
