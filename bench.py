@@ -118,6 +118,8 @@ def make_scene(args, rank):
         return scenes.dam_break_3d(seed=rank)
     if args.scene == "dam_small":
         return scenes.dam_break_3d(fluid=(40, 40, 80), box=(120, 40, 96), seed=rank)
+    if args.scene == "dam_mid":  # the 1 M-fluid scaled dam break (benchmark config 5)
+        return scenes.dam_break_3d(fluid=(80, 80, 160), box=(240, 80, 192), seed=rank)
     raise SystemExit("unknown scene " + args.scene)
 
 
@@ -170,7 +172,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--scene", default="dam", choices=["dam", "dam_small"])
+    ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=25.0)

@@ -234,6 +234,13 @@ int mph_profile_enable(mph_ctx* ctx, int enable);
  * mph_profile_enable(ctx, 1); *count receives the number of kernel names. */
 int mph_profile_read(mph_ctx* ctx, mph_kernel_stat* out, int capacity, int* count);
 
+/* Self-check of the exactly rounded FP64 division the FP64 kernels use in
+ * place of the IEEE '/' (no reference counterpart): compares it bit for bit
+ * with the hardware division on n random and adversarial operand pairs on the
+ * current device; *mismatches receives the count (0 expected) and, if any,
+ * first[0]/first[1] one failing numerator/denominator (may be NULL). */
+int mph_check_exact_division(long long n, unsigned long long seed, long long* mismatches, double* first);
+
 /* Last error message of ctx (or of the calling thread if ctx is NULL). */
 int mph_last_error(mph_ctx* ctx, char* buf, int len);
 

@@ -14,6 +14,13 @@
 // order; the file is compiled with -fmad=false and uses IEEE division and
 // square root, so each operation rounds exactly as on the CPU.
 #include "mph_internal.h"
+#include "mph_exact.cuh"
+
+// Resident 128-thread blocks per SM the sweeps are compiled for (register cap
+// 65536 / (128 * MPH_SWEEP_MINB)); latency hiding vs. spills, set by measurement.
+#ifndef MPH_SWEEP_MINB
+#define MPH_SWEEP_MINB 8
+#endif
 
 namespace mph {
 
@@ -35,10 +42,6 @@ __device__ __forceinline__ void disp(const SimConst& c, const double4& pi, const
 }
 
 // Kernel shapes, main.cpp:214-284, with q = r/h computed by division.
-__device__ __forceinline__ double f_wa(const SimConst& c, double r) {
-    const double q = r / c.ra;
-    return ((c.ca * q) * (1.0 - q)) * (1.0 - q);
-}
 __device__ __forceinline__ double f_dwadr(const SimConst& c, double r) {
     const double q = r / c.ra;
     return ((c.ca * (1.0 - q)) * (1.0 - 3.0 * q)) * c.inv_ra;
@@ -50,10 +53,6 @@ __device__ __forceinline__ double f_wg(const SimConst& c, double r) {
 __device__ __forceinline__ double f_dwgdr(const SimConst& c, double r) {
     const double q = r / c.rg;
     return c.cg * (c.m2_rg * (1.0 - q));
-}
-__device__ __forceinline__ double f_wp(const SimConst& c, double r) {
-    const double q = r / c.rp;
-    return c.cp * ((1.0 - q) * (1.0 - q));
 }
 __device__ __forceinline__ double f_dwpdr(const SimConst& c, double r) {
     const double q = r / c.rp;
@@ -127,16 +126,29 @@ k_move(SimConst c, const int* __restrict__ cellstart, double4* __restrict__ pos,
     }
 }
 
+// Kernel shapes as functions of q = r/h (main.cpp:214-284; the reference's
+// (1.0/h) factor is the rounded reciprocal inv_h, as there).
+__device__ __forceinline__ double s_wa(const SimConst& c, double q) { return ((c.ca * q) * (1.0 - q)) * (1.0 - q); }
+__device__ __forceinline__ double s_dwa(const SimConst& c, double q) {
+    return ((c.ca * (1.0 - q)) * (1.0 - 3.0 * q)) * c.inv_ra;
+}
+__device__ __forceinline__ double s_wg(const SimConst& c, double q) { return c.cg * ((1.0 - q) * (1.0 - q)); }
+__device__ __forceinline__ double s_dwg(const SimConst& c, double q) { return c.cg * (c.m2_rg * (1.0 - q)); }
+__device__ __forceinline__ double s_wp(const SimConst& c, double q) { return c.cp * ((1.0 - q) * (1.0 - q)); }
+__device__ __forceinline__ double s_dwp(const SimConst& c, double q) { return c.cp * (c.m2_rp * (1.0 - q)); }
+__device__ __forceinline__ double s_dwv(const SimConst& c, double q) { return c.cv * (c.m2_rv * (1.0 - q)); }
+
 // Sweep A: DensityA (main.cpp:1665-1692), GravityCenter (1695-1727),
 // DensityP (1831-1858), DivergenceP (1860-1896), then
 // calculatePhysicalCoefficients (1631-1662) and the PressureP / PressureA
-// values (1904-1906, 1735-1740).
+// values (1904-1906, 1735-1740).  Every division of the reference is an
+// exactly rounded div_rn (mph_exact.cuh) against one reciprocal per pair.
 template <bool ST, bool RATIO>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MPH_SWEEP_MINB)
 k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
           const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
-          double* __restrict__ strain_p, double* __restrict__ div_p, double2* __restrict__ press,
-          double4* __restrict__ gcout, double* __restrict__ wall_center) {
+          double* __restrict__ strain_p, double* __restrict__ div_p, double4* __restrict__ velp,
+          double4* __restrict__ gcpa, double* __restrict__ wall_center) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (wall_center != nullptr && blockIdx.x == 0 && threadIdx.x < 12) {
         // WallCenter += WallVelocity*Dt (main.cpp:2048-2052); the move kernel of
@@ -152,8 +164,12 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
     const size_t n = (size_t)c.n;
     double sum_a = 0.0, sum_p = 0.0, sum_d = 0.0;
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    const int* lp = nlist + i;
+    int jn = cnt > 0 ? __ldg(lp) : 0;  // next index, loaded one iteration ahead
     for (int k = 0; k < cnt; ++k) {
-        const int j = __ldg(nlist + (size_t)k * n + i);
+        const int j = jn;
+        lp += n;
+        if (k + 1 < cnt) jn = __ldg(lp);
         if (j == i) continue;
         const double4 pj = pos[j];
         double x[3];
@@ -166,20 +182,24 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
         const double r = sqrt(r2);
         double ratio = 1.0;
         if (RATIO) ratio = c.ratio[ti][type_of(pj)];
+        const double qa = div_rn(r, c.ra, c.inv_ra);
         if (in_a) {
-            const double w = RATIO ? ratio * f_wa(c, r) : f_wa(c, r);
+            const double w = RATIO ? ratio * s_wa(c, qa) : s_wa(c, qa);
             sum_a += w;
         }
         if (ST && in_g) {
-            const double w = RATIO ? ratio * f_wg(c, r) : f_wg(c, r);
-            g0 += x[0] * w / c.r2g * c.rg;
-            g1 += x[1] * w / c.r2g * c.rg;
-            g2 += x[2] * w / c.r2g * c.rg;
+            const double qg = c.rg_eq_ra ? qa : div_rn(r, c.rg, c.inv_rg);
+            const double w = RATIO ? ratio * s_wg(c, qg) : s_wg(c, qg);
+            g0 += div_rn(x[0] * w, c.r2g, c.inv_r2g) * c.rg;
+            g1 += div_rn(x[1] * w, c.r2g, c.inv_r2g) * c.rg;
+            g2 += div_rn(x[2] * w, c.r2g, c.inv_r2g) * c.rg;
         }
         if (in_p) {
-            sum_p += f_wp(c, r);
-            const double dw = f_dwpdr(c, r);
-            const double e0 = x[0] / r, e1 = x[1] / r, e2 = x[2] / r;
+            const double qp = div_rn(r, c.rp, c.inv_rp);
+            sum_p += s_wp(c, qp);
+            const double dw = s_dwp(c, qp);
+            const double ri = __drcp_rn(r);
+            const double e0 = div_rn(x[0], r, ri), e1 = div_rn(x[1], r, ri), e2 = div_rn(x[2], r, ri);
             const double4 vj = vel[j];
             const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
             sum_d -= u0 * e0 * dw;
@@ -191,14 +211,15 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
     const double strain = sum_p - c.n0p;
     strain_p[i] = strain;
     div_p[i] = sum_d;
-    if (ST) gcout[i] = make_double4(g0, g1, g2, 0.0);
     double kappa = c.bulk_modulus[ti];
     if (strain < 0.0) kappa = 0.0;
     const double lambda = c.bulk_viscosity[ti];
     const double pp = -lambda * sum_d + kappa * strain;
     double pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
     if (c.n0a <= sum_a) pa = 0.0;
-    press[i] = make_double2(pp, pa);
+    // sweep B gathers {v, PressureP} and {GravityCenter, PressureA} per neighbour
+    velp[i] = make_double4(vi.x, vi.y, vi.z, pp);
+    gcpa[i] = make_double4(g0, g1, g2, pa);
 }
 
 // Sweep B: PressureP force (main.cpp:1908-1938), PressureA force
@@ -206,93 +227,101 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
 // reference), ViscosityV (1943-1984); Force = 0 + fP + fA + fDI + fV, then
 // Gravity (1988-1998) and Acceleration (2000-2010) for fluid particles.
 template <bool ST, bool RATIO>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, MPH_SWEEP_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
-          const double4* __restrict__ vel, double4* __restrict__ vel_out, const double2* __restrict__ press,
-          const double4* __restrict__ gc, const int* __restrict__ ncount, const int* __restrict__ nlist,
-          double4* __restrict__ force, StepScalars* __restrict__ scal) {
+          const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
+          const int* __restrict__ ncount, const int* __restrict__ nlist, double4* __restrict__ force,
+          StepScalars* __restrict__ scal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const double4 pi = pos[i];
-    const double4 vi = vel[i];
-    const double2 pri = press[i];
+    const double4 vi = velp[i];   // .w = PressureP
     const int ti = type_of(pi);
-    const double mui = c.shear_viscosity[ti];
     const double ai = c.a_k[ti];
     double4 gci = make_double4(0, 0, 0, 0);
-    if (ST) gci = gc[i];
+    if (ST) gci = gcpa[i];        // .w = PressureA
     const int cnt = ncount[i];
     const size_t n = (size_t)c.n;
     double fp0 = 0.0, fp1 = 0.0, fp2 = 0.0;
     double fa0 = 0.0, fa1 = 0.0, fa2 = 0.0;
     double fd0 = 0.0, fd1 = 0.0, fd2 = 0.0;
     double fv0 = 0.0, fv1 = 0.0, fv2 = 0.0;
+    const int* lp = nlist + i;
+    int jn = cnt > 0 ? __ldg(lp) : 0;  // next index, loaded one iteration ahead
     for (int k = 0; k < cnt; ++k) {
-        const int j = __ldg(nlist + (size_t)k * n + i);
+        const int j = jn;
+        lp += n;
+        if (k + 1 < cnt) jn = __ldg(lp);
         if (j == i) continue;
         const double4 pj = pos[j];
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        // Without surface tension every CofA is 0, PressureA is +-0 and each
+        // PressureA term adds a signed zero to a sum that starts at +0: the sum
+        // stays +0 exactly, so the term is skipped (ST == false).
         const bool in_p = c.rp2 - r2 > 0;
-        const bool in_a = c.ra2 - r2 > 0;
+        const bool in_a = ST && (c.ra2 - r2 > 0);
         const bool in_g = ST && (c.rg2 - r2 > 0);
         const bool in_v = c.rv2 - r2 > 0;
         if (!(in_p || in_a || in_g || in_v)) continue;
         const int tj = type_of(pj);
         const double r = sqrt(r2);
-        const double e0 = x[0] / r, e1 = x[1] / r, e2 = x[2] / r;
+        const double ri = __drcp_rn(r);
+        const double e0 = div_rn(x[0], r, ri), e1 = div_rn(x[1], r, ri), e2 = div_rn(x[2], r, ri);
+        const double qa = div_rn(r, c.ra, c.inv_ra);
         double rij = 1.0, rji = 1.0;
         if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
+        const double4 vj = velp[j];   // .w = PressureP of j
         if (in_p) {
-            const double prj = press[j].x;
-            const double dw = f_dwpdr(c, r);
-            const double gw0 = dw * x[0] / r, gw1 = dw * x[1] / r, gw2 = dw * x[2] / r;
-            const double ps = pri.x + prj;
+            const double qp = div_rn(r, c.rp, c.inv_rp);
+            const double dw = s_dwp(c, qp);
+            const double gw0 = div_rn(dw * x[0], r, ri), gw1 = div_rn(dw * x[1], r, ri),
+                         gw2 = div_rn(dw * x[2], r, ri);
+            const double ps = vi.w + vj.w;
             fp0 += ps * gw0 * c.vol;
             fp1 += ps * gw1 * c.vol;
             fp2 += ps * gw2 * c.vol;
         }
         if (in_a) {
-            const double paj = press[j].y;
-            const double dwa = f_dwadr(c, r);
+            const double dwa = s_dwa(c, qa);
             const double dwij = RATIO ? rij * dwa : dwa;
             const double dwji = RATIO ? rji * dwa : dwa;
-            const double s = pri.y * dwij + paj * dwji;
+            const double s = gci.w * dwij + gcpa[j].w * dwji;
             fa0 += s * e0 * c.vol;
             fa1 += s * e1 * c.vol;
             fa2 += s * e2 * c.vol;
         }
         if (ST && in_g) {
-            const double4 gcj = gc[j];
+            const double4 gcj = gcpa[j];
             const double aj = ai;
-            const double wg = f_wg(c, r);
+            const double qg = c.rg_eq_ra ? qa : div_rn(r, c.rg, c.inv_rg);
+            const double wg = s_wg(c, qg);
             const double wij = RATIO ? rij * wg : wg;
             const double wji = RATIO ? rji * wg : wg;
-            fd0 -= (aj * gcj.x * wji - ai * gci.x * wij) / c.r2g * c.rg * c.vol_over_l0;
-            fd1 -= (aj * gcj.y * wji - ai * gci.y * wij) / c.r2g * c.rg * c.vol_over_l0;
-            fd2 -= (aj * gcj.z * wji - ai * gci.z * wij) / c.r2g * c.rg * c.vol_over_l0;
-            const double dg = f_dwgdr(c, r);
+            fd0 -= div_rn(aj * gcj.x * wji - ai * gci.x * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd1 -= div_rn(aj * gcj.y * wji - ai * gci.y * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd2 -= div_rn(aj * gcj.z * wji - ai * gci.z * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            const double dg = s_dwg(c, qg);
             const double dwij = RATIO ? rij * dg : dg;
             const double dwji = RATIO ? rji * dg : dg;
             double gr = 0.0;
             gr += (aj * gcj.x * dwji - ai * gci.x * dwij) * x[0];
             gr += (aj * gcj.y * dwji - ai * gci.y * dwij) * x[1];
             gr += (aj * gcj.z * dwji - ai * gci.z * dwij) * x[2];
-            fd0 -= (gr) * e0 / c.r2g * c.rg * c.vol_over_l0;
-            fd1 -= (gr) * e1 / c.r2g * c.rg * c.vol_over_l0;
-            fd2 -= (gr) * e2 / c.r2g * c.rg * c.vol_over_l0;
+            fd0 -= div_rn((gr) * e0, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd1 -= div_rn((gr) * e1, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd2 -= div_rn((gr) * e2, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
         }
         if (in_v) {
-            const double dw = -f_dwvdr(c, r);
-            const double4 vj = vel[j];
+            const double qv = c.rv_eq_ra ? qa : div_rn(r, c.rv, c.inv_rv);
+            const double dw = -s_dwv(c, qv);
             const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
-            const double muj = c.shear_viscosity[tj];
-            const double muij = 2.0 * (mui * muj) / (mui + muj);
+            const double cm = c.visc_mu[ti][tj];
             const double dot = u0 * e0 + u1 * e1 + u2 * e2;
-            fv0 += c.visc_c * muij * dot * e0 * dw / r * c.vol;
-            fv1 += c.visc_c * muij * dot * e1 * dw / r * c.vol;
-            fv2 += c.visc_c * muij * dot * e2 * dw / r * c.vol;
+            fv0 += div_rn(cm * dot * e0 * dw, r, ri) * c.vol;
+            fv1 += div_rn(cm * dot * e1 * dw, r, ri) * c.vol;
+            fv2 += div_rn(cm * dot * e2 * dw, r, ri) * c.vol;
         }
     }
     double F0 = 0.0, F1 = 0.0, F2 = 0.0;   // resetForce (main.cpp:1617-1628)
@@ -300,7 +329,7 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     F0 += fa0; F1 += fa1; F2 += fa2;
     F0 += fd0; F1 += fd1; F2 += fd2;
     F0 += fv0; F1 += fv1; F2 += fv2;
-    double4 vn = vi;
+    double4 vn = make_double4(vi.x, vi.y, vi.z, 0.0);
     const int nf = cellstart[c.tot];
     if (i < nf) {
         const double m = c.density[ti] * c.vol;
@@ -316,19 +345,47 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     vel_out[i] = vn;
 }
 
+// Self-check of div_rn against the hardware IEEE division: operands with
+// random significands and exponents in [-40, 40], plus all-ones significands.
+__global__ void k_check_division(unsigned long long seed, long long n, unsigned long long* mismatches,
+                                 double* first) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += stride) {
+        unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(t + 1);
+        auto mix = [](unsigned long long v) {
+            v ^= v >> 30; v *= 0xBF58476D1CE4E5B9ull;
+            v ^= v >> 27; v *= 0x94D049BB133111EBull;
+            return v ^ (v >> 31);
+        };
+        const unsigned long long a = mix(z), b = mix(z ^ 0xD1B54A32D192ED03ull), e = mix(z + 17);
+        unsigned long long ma = a & 0xFFFFFFFFFFFFFull, mb = b & 0xFFFFFFFFFFFFFull;
+        if ((e & 15) == 0) mb = 0xFFFFFFFFFFFFFull;
+        if ((e & 15) == 1) ma = 0xFFFFFFFFFFFFFull;
+        const int ea = (int)((e >> 8) % 81) - 40, eb = (int)((e >> 20) % 81) - 40;
+        const unsigned long long sa = (e >> 40) & 1ull;
+        const double x = __longlong_as_double((long long)((sa << 63) | ((unsigned long long)(1023 + ea) << 52) | ma));
+        const double y = __longlong_as_double((long long)(((unsigned long long)(1023 + eb) << 52) | mb));
+        const double q = div_rn(x, y, __drcp_rn(y));
+        const double ref = x / y;
+        if (__double_as_longlong(q) != __double_as_longlong(ref)) {
+            if (atomicAdd(mismatches, 1ull) == 0) { first[0] = x; first[1] = y; }
+        }
+    }
+}
+
 // Virial stress at particles, main.cpp:2057-2302: four sums (PressureP,
 // PressureA, ViscosityV, DiffuseInterface) added in that order.
 __global__ void __launch_bounds__(128)
 k_virial(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
-         const double2* __restrict__ press, const double4* __restrict__ gc, const int* __restrict__ ncount,
+         const double4* __restrict__ velp, const double4* __restrict__ gc, const int* __restrict__ ncount,
          const int* __restrict__ nlist, double* __restrict__ virial_p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const double4 pi = pos[i];
     const double4 vi = vel[i];
     const int ti = type_of(pi);
-    const double2 pri = press[i];
-    const double4 gci = gc ? gc[i] : make_double4(0, 0, 0, 0);
+    const double2 pri = make_double2(velp[i].w, gc[i].w);   // {PressureP, PressureA}
+    const double4 gci = gc[i];
     const double mui = c.shear_viscosity[ti];
     const int cnt = ncount[i];
     const size_t n = (size_t)c.n;
@@ -438,7 +495,7 @@ void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4*
 
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,
                     const int* ncount, const int* nlist, int cap_stride, double* dens_a, double* strain_p,
-                    double* div_p, double2* press, double4* gc, double* wall_center, cudaStream_t s) {
+                    double* div_p, double4* press, double4* gc, double* wall_center, cudaStream_t s) {
     (void)cellstart;
     (void)cap_stride;
     const int nb = blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1;
@@ -456,25 +513,31 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
 }
 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
-                    double4* vel_out, const double2* press, const double4* gc, const int* ncount,
+                    double4* vel_out, const double4* press, const double4* gc, const int* ncount,
                     const int* nlist, double4* force, StepScalars* scal, cudaStream_t s) {
     const int nb = blocks(c.n, 128);
     if (c.has_st) {
         if (c.ratio_all_one)
-            k_sweep_b<true, false><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+            k_sweep_b<true, false><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
         else
-            k_sweep_b<true, true><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+            k_sweep_b<true, true><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
     } else {
         if (c.ratio_all_one)
-            k_sweep_b<false, false><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+            k_sweep_b<false, false><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
         else
-            k_sweep_b<false, true><<<nb, 128, 0, s>>>(c, cellstart, pos, vel_in, vel_out, press, gc, ncount, nlist, force, scal);
+            k_sweep_b<false, true><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
     }
 }
 
-void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double2* press,
+void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double4* press,
                    const double4* gc, const int* ncount, const int* nlist, double* virial_p, cudaStream_t s) {
     k_virial<<<blocks(c.n, 128), 128, 0, s>>>(c, pos, vel, press, gc, ncount, nlist, virial_p);
+}
+
+int check_division(unsigned long long seed, long long n, unsigned long long* d_count, double* d_first,
+                   cudaStream_t s) {
+    k_check_division<<<148 * 8, 256, 0, s>>>(seed, n, d_count, d_first);
+    return 1;
 }
 
 void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,

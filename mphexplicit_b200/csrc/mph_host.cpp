@@ -271,6 +271,15 @@ static int fill_simconst(mph_ctx* ctx) {
     s.inv_ra = 1.0 / s.ra; s.inv_rg = 1.0 / s.rg; s.inv_rp = 1.0 / s.rp; s.inv_rv = 1.0 / s.rv;
     s.m2_rg = -2.0 / s.rg; s.m2_rp = -2.0 / s.rp; s.m2_rv = -2.0 / s.rv;
     s.visc_c = dim == 2 ? 8.0 : 10.0;
+    s.inv_r2g = 1.0 / s.r2g;
+    s.rg_eq_ra = s.rg == s.ra;
+    s.rv_eq_ra = s.rv == s.ra;
+    for (int t = 0; t < MPH_TYPE_COUNT; ++t)
+        for (int u = 0; u < MPH_TYPE_COUNT; ++u) {
+            const double mi = p.shear_viscosity[t], mj = p.shear_viscosity[u];
+            const double muij = 2.0 * (mi * mj) / (mi + mj);
+            s.visc_mu[t][u] = s.visc_c * muij;
+        }
     const double margin = 0.1 * l0;
     s.shift_thr = 0.5 * margin * 0.5 * margin;  // main.cpp:1102
     s.has_st = 0;
@@ -683,13 +692,14 @@ extern "C" int mph_get_fields(mph_ctx* ctx, double* divergence_p, double* pressu
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     TRY(d2h(ctx, divergence_p, d.div_p, n));
-    if (pressure_p || pressure_a) {
-        std::vector<double2> pr(n);
-        CUDA_TRY(ctx, cudaMemcpyAsync(pr.data(), d.press, n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    if (pressure_p || pressure_a) {  // PressureP rides in velp.w, PressureA in gc.w
+        std::vector<double4> vp(n), ga(n);
+        CUDA_TRY(ctx, cudaMemcpyAsync(vp.data(), d.press, n * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(ga.data(), d.gc, n * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
         CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         for (size_t i = 0; i < n; ++i) {
-            if (pressure_p) pressure_p[i] = pr[i].x;
-            if (pressure_a) pressure_a[i] = pr[i].y;
+            if (pressure_p) pressure_p[i] = vp[i].w;
+            if (pressure_a) pressure_a[i] = ga[i].w;
         }
     }
     if (gravity_center) TRY(d2h_vec3(ctx, d.gc, gravity_center));
@@ -805,6 +815,31 @@ extern "C" int mph_conserved_sums(mph_ctx* ctx, double out[5]) {
     for (int k = 0; k < 5; ++k) out[k] = 0.0;
     for (int b = 0; b < nb; ++b)
         for (int k = 0; k < 5; ++k) out[k] += h[5 * (size_t)b + k];
+    return MPH_OK;
+}
+
+extern "C" int mph_check_exact_division(long long n, unsigned long long seed, long long* mismatches,
+                                        double* first) {
+    if (!mismatches || n < 0) return fail(nullptr, MPH_ERR_ARG, "bad arguments");
+    unsigned long long* d_count = nullptr;
+    double* d_first = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d_count, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_first, 2 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(d_count, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d_first, 0, 2 * sizeof(double));
+    if (e == cudaSuccess) {
+        mph::check_division(seed, n, d_count, d_first, 0);
+        e = cudaGetLastError();
+    }
+    unsigned long long cnt = 0;
+    double f[2] = {0.0, 0.0};
+    if (e == cudaSuccess) e = cudaMemcpy(&cnt, d_count, sizeof(cnt), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(f, d_first, sizeof(f), cudaMemcpyDeviceToHost);
+    if (d_count) cudaFree(d_count);
+    if (d_first) cudaFree(d_first);
+    if (e != cudaSuccess) return fail(nullptr, MPH_ERR_CUDA, cudaGetErrorString(e));
+    *mismatches = (long long)cnt;
+    if (first) { first[0] = f[0]; first[1] = f[1]; }
     return MPH_OK;
 }
 

@@ -34,6 +34,10 @@ struct SimConst {
     double inv_ra, inv_rg, inv_rp, inv_rv;  // 1.0/h
     double m2_rg, m2_rp, m2_rv;        // -2.0/h
     double visc_c;                     // 8 (2-D) or 10 (3-D)
+    double inv_r2g;                    // RN(1/R2g)
+    int rg_eq_ra, rv_eq_ra;            // radii equal: r/h shared
+    // visc_c * muij per type pair, muij = 2*(mu_i*mu_j)/(mu_i+mu_j) (main.cpp:1968)
+    double visc_mu[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
     double shift_thr;                  // 0.5*MARGIN*0.5*MARGIN
     double density[MPH_TYPE_COUNT], bulk_modulus[MPH_TYPE_COUNT];
     double bulk_viscosity[MPH_TYPE_COUNT], shear_viscosity[MPH_TYPE_COUNT];
@@ -72,8 +76,8 @@ struct DevFP64 {
     double* dens_a = nullptr;
     double* strain_p = nullptr;
     double* div_p = nullptr;
-    double2* press = nullptr;               // {PressureP, PressureA}
-    double4* gc = nullptr;                  // GravityCenter
+    double4* press = nullptr;               // {vx, vy, vz, PressureP} before the acceleration
+    double4* gc = nullptr;                  // {GravityCenter, PressureA}
     double* virial_p = nullptr;
     int* keys = nullptr;                    // CellIndex (sorted), pow2 entries
     int* vals = nullptr;                    // CellParticle, pow2 entries
@@ -106,14 +110,16 @@ void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4*
                  cudaStream_t s);
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel, const int* ncount, const int* nlist, int cap_stride,
-                    double* dens_a, double* strain_p, double* div_p, double2* press, double4* gc,
+                    double* dens_a, double* strain_p, double* div_p, double4* press, double4* gc,
                     double* wall_center, cudaStream_t s);
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
-                    const double4* vel_in, double4* vel_out, const double2* press,
+                    const double4* vel_in, double4* vel_out, const double4* press,
                     const double4* gc, const int* ncount, const int* nlist, double4* force,
                     StepScalars* scal, cudaStream_t s);
-void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double2* press,
+void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double4* press,
                    const double4* gc, const int* ncount, const int* nlist, double* virial_p,
+                   cudaStream_t s);
+int check_division(unsigned long long seed, long long n, unsigned long long* d_count, double* d_first,
                    cudaStream_t s);
 void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos,
                       const double4* vel, double* out5, cudaStream_t s);

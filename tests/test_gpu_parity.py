@@ -177,3 +177,14 @@ def test_full_size_dam_break_two_steps():
         assert_same(a[key], b[key], key)
     fluid = a["type"] < 2
     assert np.median(a["neighbor_count"][fluid]) >= 180
+
+
+def test_exact_division_matches_hardware_ieee():
+    """The FP64 kernels divide with div_rn (Markstein's method on a correctly
+    rounded reciprocal); it must equal the hardware IEEE quotient bit for bit."""
+    import ctypes as C
+    lib = N.load()
+    mism = C.c_longlong(-1)
+    first = (C.c_double * 2)()
+    assert lib.mph_check_exact_division(10_000_000_000, 12345, C.byref(mism), first) == 0
+    assert mism.value == 0, (mism.value, first[0], first[1])
