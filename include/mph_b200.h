@@ -241,6 +241,32 @@ int mph_profile_read(mph_ctx* ctx, mph_kernel_stat* out, int capacity, int* coun
  * first[0]/first[1] one failing numerator/denominator (may be NULL). */
 int mph_check_exact_division(long long n, unsigned long long seed, long long* mismatches, double* first);
 
+/* Cell sort without any allocation.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc -- their device memory belongs to
+ * another allocator (a framework's caching allocator, a pool with a fixed
+ * budget) or they run a time-critical loop where allocating, and cudaFree's
+ * device synchronisation, are not allowed.  It computes what the reference's
+ * calculateCellParticle computes (main.cpp:1111-1247) for n particles in file
+ * order: the sorted CellIndex (cell_index[n]), the bitonic permutation
+ * CellParticle (cell_particle[n]) and the per-cell ranges as
+ * cell_start[2*total_cell_count+1] (number of sorted keys below each key value:
+ * fluid cell c spans [cell_start[c], cell_start[c+1]), wall cell c spans
+ * [cell_start[c+T], cell_start[c+T+1]) with T = total_cell_count).
+ * xyz (double[n][3]), type, and the three outputs are DEVICE pointers owned by
+ * the caller; c comes from mph_compute_constants, h gives the domain origin;
+ * stream is a cudaStream_t (NULL: the legacy default stream) and the call is
+ * asynchronous on it.  The sort's scratch is a fixed static device array of
+ * 2^21 ints (8 MiB, held by every GPU that loads the library until exit), so
+ * n must be below 2^20 (1,048,576); larger n returns MPH_ERR_CAPACITY.  The
+ * first call on a device looks up that array's device address (set-up), so
+ * make that first call before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Allocates nothing
+ * (no cudaMalloc, cudaFree or allocating library call). */
+int mph_cell_sort_noalloc(const mph_constants* c, const mph_grid_header* h, int n,
+                          const double* xyz, const int* type, int* cell_index,
+                          int* cell_particle, int* cell_start, void* stream);
+
 /* Last error message of ctx (or of the calling thread if ctx is NULL). */
 int mph_last_error(mph_ctx* ctx, char* buf, int len);
 

@@ -154,6 +154,7 @@ SIGNATURES = {
     "mph_profile_enable": (_I, [_P, _I]),
     "mph_profile_read": (_I, [_P, C.POINTER(KernelStat), _I, _ip]),
     "mph_check_exact_division": (_I, [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong), _dp]),
+    "mph_cell_sort_noalloc": (_I, [C.POINTER(Constants), C.POINTER(GridHeader), _I, _P, _P, _P, _P, _P, _P]),
     "mph_last_error": (_I, [_P, C.c_char_p, _I]),
     "mph_destroy": (None, [_P]),
     "mph_version": (C.c_char_p, []),

@@ -110,6 +110,8 @@ static int fail(mph_ctx* ctx, int code, const std::string& msg) {
     return code;
 }
 
+int mph::set_thread_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+
 #define CUDA_TRY(ctx, expr)                                                                \
     do {                                                                                   \
         cudaError_t e_ = (expr);                                                           \

@@ -124,4 +124,7 @@ int check_division(unsigned long long seed, long long n, unsigned long long* d_c
 void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos,
                       const double4* vel, double* out5, cudaStream_t s);
 
+// Sets the calling thread's message for mph_last_error(NULL, ...) and returns code.
+int set_thread_error(int code, const std::string& msg);
+
 }  // namespace mph
