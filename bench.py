@@ -12,7 +12,7 @@ A "step" is one explicit step of the whole scene (the reference's loop body).
 value = fluid particles x steps / seconds, summed over ranks (replicas: the
 step does not shard, each rank runs its own scene on its own GPU).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed|mixed_p64] [--only]
   python bench.py --impl reference ...   # the reference's own CPU step, all host threads
 
 One JSON line on rank 0.
@@ -39,7 +39,8 @@ UNIT = "particle-updates/s"
 # algorithmic HBM bytes per particle per launch, 3-D without surface tension:
 # sweep A reads x, v, type (52 B) and writes PressureP (8 B); sweep B reads
 # x, v, type, PressureP (60 B) and writes x, v (48 B)  -> 168 B per update.
-ALGO_BYTES = {"sweep_a": 60.0, "sweep_b": 108.0, "move": 96.0}
+ALGO_BYTES = {"sweep_a": 60.0, "sweep_b": 108.0, "mix_sweep_a": 60.0, "mix_sweep_b": 108.0, "move": 96.0,
+              "mix_move": 96.0}
 
 
 def dist_env():
@@ -165,13 +166,98 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def measure_form(args, sc, mode, world, gpu_index, with_e2e):
+    """Time one form of the step on the bench scene: device-resident timed
+    region (CUDA events on the library stream), per-kernel events, clocks;
+    optionally the end-to-end path with host buffers."""
+    import torch
+    import torch.distributed as dist
+    import mphexplicit_b200 as M
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim, mode=mode)
+    warm = max(args.warmup, 3)
+    s.step(warm)
+    s.synchronize()
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s.profile(True)
+    l0 = s.launch_count()
+    info0 = s.info()
+    with ClockSampler(gpu_index) as clk:
+        ev0.record(stream)
+        s.step(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.launch_count() - l0
+    prof = s.profile_read()
+    s.profile(False)
+    info1 = s.info()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = s.state()  # after warm + steps, for the cross-form error
+    order = np.argsort(st["particle_index"], kind="stable")
+    vel = st["vel"][order]
+    fluid = st["type"][order] < 2
+    n_fluid, n_all = sc.n_fluid, sc.n
+    out = {"mode": mode, "ms": ms, "value": n_fluid * args.steps * world / (ms / 1e3), "launches": launches,
+           "prof": prof, "clocks": clk.summary(), "rebuilds": info1["rebuild_count"] - info0["rebuild_count"],
+           "vel": vel, "fluid": fluid}
+    # roofline of the dominant kernel: algorithmic bytes per particle the
+    # kernel updates (FP64 state, neighbour re-reads on chip)
+    name, (nl, tot_ms) = max(prof.items(), key=lambda kv: kv[1][1])
+    avg_s = tot_ms / nl / 1e3
+    peak, peak_kind = measured_peaks()
+    units = n_fluid if name == "mix_sweep_b" else n_all
+    algo = ALGO_BYTES.get(name, 0.0) * units
+    achieved = algo / avg_s / 1e9
+    out["roofline"] = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "traffic": ncu_traffic(name), "peak_source": peak_kind,
+                       "algorithmic_bytes_per_launch": algo, "particles_per_launch": units,
+                       "avg_launch_ms": avg_s * 1e3,
+                       "kernels_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
+    if with_e2e:
+        ke = max(1, args.e2e_steps)
+        hx = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
+        hv = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
+        s.get_xv(hx, hv)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        for _ in range(ke):
+            s.set_state(hx, hv)
+            s.step(1)
+            s.get_xv(hx, hv)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        out["e2e"] = {"value": n_fluid * ke * world / (e2e_ms / 1e3), "unit": UNIT,
+                      "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes),
+                      "d2h_bytes_per_step": int(hx.nbytes + hv.nbytes), "steps": ke, "mode": mode}
+    s.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mode", default="mixed_p64", choices=["fp64", "mixed", "mixed_p64"],
+                    help="headline form (all three are measured unless --only)")
+    ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -192,99 +278,45 @@ def main():
         return
 
     torch.cuda.set_device(local)
-    import mphexplicit_b200 as M
-    sc = make_scene(args, rank)
-    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim, mode=args.mode)
-    s.step(max(args.warmup, 3))
-    s.synchronize()
-    stream = torch.cuda.ExternalStream(s.stream_handle)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-
-    # ---- device-resident timed region ----------------------------------
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
     gpu_index = local
     cvd = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     if cvd and "," not in cvd and cvd.isdigit():
         gpu_index = int(cvd)
-    s.profile(True)
-    l0 = s.launch_count()
-    info0 = s.info()
-    with ClockSampler(gpu_index) as clk:
-        ev0.record(stream)
-        s.step(args.steps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = s.launch_count() - l0
-    prof = s.profile_read()
-    s.profile(False)
-    info1 = s.info()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    n_fluid, n_all = sc.n_fluid, sc.n
-    value = n_fluid * args.steps * world / (ms / 1e3)
-
-    # roofline of the dominant kernel
-    dom = max(prof.items(), key=lambda kv: kv[1][1])
-    name, (nl, tot_ms) = dom
-    avg_s = tot_ms / nl / 1e3
-    peak, peak_kind = measured_peaks()
-    algo = ALGO_BYTES.get(name, 0.0) * n_all
-    achieved = algo / avg_s / 1e9
-    roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": ncu_traffic(name), "peak_source": peak_kind,
-            "algorithmic_bytes_per_launch": algo, "avg_launch_ms": avg_s * 1e3,
-            "kernels_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
-
-    # ---- end to end through the C ABI with host buffers ------------------
-    ke = max(1, args.e2e_steps)
-    hx = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
-    hv = torch.empty((n_all, 3), dtype=torch.float64, pin_memory=True).numpy()
-    s.get_xv(hx, hv)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ev0.record(stream)
-    for _ in range(ke):
-        s.set_state(hx, hv)
-        s.step(1)
-        s.get_xv(hx, hv)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - t0
-    e2e_ms = max(ev0.elapsed_time(ev1), e2e_wall * 1e3)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": n_fluid * ke * world / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes), "d2h_bytes_per_step": int(hx.nbytes + hv.nbytes),
-           "steps": ke}
+    sc = make_scene(args, rank)
+    modes = [args.mode] if args.only else ["fp64", "mixed", "mixed_p64"]
+    res = {m: measure_form(args, sc, m, world, gpu_index, with_e2e=(m == args.mode)) for m in modes}
+    head = res[args.mode]
+    forms = {}
+    for m, r in res.items():
+        f = {"value": r["value"], "ms_per_step": r["ms"] / args.steps, "dominant_kernel": r["roofline"]["kernel"],
+             "kernels_ms_per_step": r["roofline"]["kernels_ms_per_step"], "rebuilds_in_timed_region": r["rebuilds"]}
+        if "fp64" in res and m != "fp64":
+            ref = res["fp64"]
+            fl = ref["fluid"]
+            f["rel_l2_vel_vs_fp64"] = float(np.linalg.norm(r["vel"][fl] - ref["vel"][fl]) /
+                                           np.linalg.norm(ref["vel"][fl]))
+            f["error_steps"] = max(args.warmup, 3) + args.steps
+            f["speedup_vs_fp64"] = ref["ms"] / r["ms"]
+        forms[m] = f
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(sc, args.ref_seconds, args.ref_max_steps)
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32/f64",
+        n_all = sc.n
+        line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32+f64",
                 "data": "synthetic (seeded generator)",
                 "config": {"workload": workload_name(sc), "mode": args.mode,
                            "parallelism": "replicas" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2 (%.2f GB device state)" % (n_all * 260 / 1e9),
-                           "rebuilds_in_timed_region": info1["rebuild_count"] - info0["rebuild_count"],
-                           "updates_all_particles_per_s": n_all * args.steps * world / (ms / 1e3)},
-                "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary()}
+                           "rebuilds_in_timed_region": head["rebuilds"],
+                           "updates_all_particles_per_s": n_all * args.steps * world / (head["ms"] / 1e3)},
+                "forms": forms, "roofline": head["roofline"], "cpu_baseline": base, "e2e": head["e2e"],
+                "gpu_launches": head["launches"], "clocks": head["clocks"]}
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         dist.destroy_process_group()
 

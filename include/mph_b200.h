@@ -48,6 +48,10 @@ extern "C" {
  * per-particle sums; FP64 position/velocity integration; counting-sort cell
  * lists rebuilt every step (no stored neighbour list). */
 #define MPH_MODE_MIXED    1
+/* The mixed form with its short-range pressure pairs (DensityP, DivergenceP
+ * and the PressureP force, ~12% of the pairs) in FP64 and the long-range
+ * pairs (viscosity, surface tension) in FP32. */
+#define MPH_MODE_MIXED_P64 2
 
 /* ---- parameters read from the *.data file (main.cpp:489-539) --------- */
 typedef struct mph_params {

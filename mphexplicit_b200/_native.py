@@ -24,6 +24,7 @@ MPH_ERR_GEOMETRY = -9
 
 MODE_FP64 = 0
 MODE_MIXED = 1
+MODE_MIXED_P64 = 2
 
 _D4 = C.c_double * TYPE_COUNT
 _D44 = (C.c_double * TYPE_COUNT) * TYPE_COUNT

@@ -1,24 +1,1005 @@
-// k_mixed.cu — mixed-precision form (placeholder until the kernels land).
+// k_mixed.cu — the mixed-precision MPH-WC step on sm_100a.
+//
+// Same physics and step order as the reference loop (main.cpp:386-431), with
+//   * a stable counting sort by cell (histogram -> scan -> scatter -> in-cell
+//     ordering by previous index) instead of the bitonic network;
+//   * FP32 pair arithmetic on cell-relative coordinates: each particle keeps
+//     its FP32 offset from the origin of its home cell (the cell of the last
+//     list build), and every list entry packs the neighbour index with a 5-bit
+//     code of the neighbouring cell's offset, so x_j - x_i = (o_j - o_i) +
+//     D[code] never subtracts two large FP32 coordinates;
+//   * one neighbour table, entries within RP+margin first, so the density
+//     sweep walks the short part only; the force sweep runs for fluid
+//     particles only (walls never accelerate);
+//   * Kahan-compensated FP32 per-particle sums; FP64 position/velocity
+//     integration, FP64 global sums.
+// Quantities the reference computes for output only (DensityA without surface
+// tension, wall forces) are computed when the state is read back.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
 #include "mph_mixed.h"
 
 namespace mph {
 
-struct MixedState {
-    long long rebuilds = 0;
+namespace {
+
+constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
+
+struct MixConst {
+    int n, tot, dim, has_st, ratio_all_one, uniform_mu;
+    int cc[3], range[3];
+    double grid, inv_grid;             // hi-part grid (a power of two, metres)
+    float dhi[27][4];                  // cell-origin offset per code: hi part (on the grid)
+    float dlo[27][4];                  //                              lo part
+    float list_r2, short_r2;           // (MaxRadius+m)^2, (RP+m)^2
+    float ra2, rp2, rv2, rg2;
+    float inv_ra, inv_rp, inv_rv, inv_rg;
+    float ca, cp, cg, cv;              // (1/Sw)/h^D
+    float cp_m2, cg_m2, cv_m2, ca_inv; // c*(-2/h); ca/h
+    float p_a, p_b;                    // pressure:  cp*(-2/rp)*vol * (1 - r/rp) = p_a + p_b*r
+    float v_a, v_b;                    // viscosity: -cv*(-2/rv)*vol * (1 - r/rv) = v_a + v_b*r
+    float vol, vol_over_l0, n0a, n0p, inv_r2g_rg, l0;
+    double p_a_d, p_b_d, v_a_d, v_b_d, cp_d, cp_m2_d, inv_rp_d, n0p_d;  // FP64 pressure core
+    float visc_mu[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
+    float ratio[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
+    float a_k[MPH_TYPE_COUNT], cof_a[MPH_TYPE_COUNT];
+    float bulk_modulus[MPH_TYPE_COUNT], bulk_viscosity[MPH_TYPE_COUNT];
 };
 
-int mixed_create(MixedState** out, const SimConst&, const mph_constants&, DevFP64&, cudaStream_t, std::string* err) {
+__device__ __forceinline__ double omod(double x, double w) { return x - w * floor(x / w); }
+__device__ __forceinline__ double omod_fast(double x, double w) {
+    return (x >= 0.0 && x < 0.75 * w) ? x : omod(x, w);
+}
+
+// Kahan-compensated accumulation (Kahan 1965): s + t with the lost low-order
+// part carried in c; the compensated value is s - c.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
+    const float y = t - c;
+    const float u = s + y;
+    c = (u - s) - y;
+    s = u;
+}
+
+__device__ __forceinline__ int pack_cell(int x, int y, int z) { return x | (y << 10) | (z << 20); }
+
+// Cell-relative position in two FP32 words.  hi lies on a power-of-two grid g
+// with |hi| < 2^24 g, so hi_j - hi_i + Dhi (also on the grid) is computed
+// exactly; lo = x - hi (|lo| <= g/2) carries the rest.  The pair
+// displacement ((hi_j - hi_i) + Dhi) + ((lo_j - lo_i) + Dlo) is then the true
+// displacement rounded once to FP32, independent of where the cell sits.
+__device__ __forceinline__ void rel32(const SimConst& c, const MixConst& m, const double4& p, int h, float4& hi,
+                                      float4& lo) {
+    const int hx = h & 1023, hy = (h >> 10) & 1023, hz = (h >> 20) & 1023;
+    double d[3] = {p.x - (c.dmin[0] + (double)hx * c.cell_width[0]), p.y - (c.dmin[1] + (double)hy * c.cell_width[1]),
+                   p.z - (c.dmin[2] + (double)hz * c.cell_width[2])};
+    float h3[3], l3[3];
+    for (int k = 0; k < 3; ++k) {
+        if (d[k] > c.half_width[k]) d[k] -= c.width[k];  // minimum image from the home cell
+        if (d[k] < -c.half_width[k]) d[k] += c.width[k];
+        const double q = rint(d[k] * m.inv_grid) * m.grid;
+        h3[k] = (float)q;
+        l3[k] = (float)(d[k] - q);
+    }
+    hi = make_float4(h3[0], h3[1], h3[2], __int_as_float((int)p.w));
+    lo = make_float4(l3[0], l3[1], l3[2], 0.0f);
+}
+
+// ---- counting sort by cell ------------------------------------------------
+
+// Cell key of main.cpp:1115-1133 (walls offset by TotalCellCount), its slot in
+// the cell (atomic, order fixed later), the cell histogram.
+__global__ void k_mix_cellkey(SimConst c, const double4* __restrict__ pos, int* __restrict__ keys,
+                              int* __restrict__ slot, int* __restrict__ counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const double4 p = pos[i];
+    const int cx = ((int)floor((p.x - c.dmin[0]) / c.cell_width[0])) % c.cc[0];
+    const int cy = ((int)floor((p.y - c.dmin[1]) / c.cell_width[1])) % c.cc[1];
+    const int cz = ((int)floor((p.z - c.dmin[2]) / c.cell_width[2])) % c.cc[2];
+    int id = ((cx % c.cc[0] + c.cc[0]) % c.cc[0]) * c.cc[1] * c.cc[2] +
+             ((cy % c.cc[1] + c.cc[1]) % c.cc[1]) * c.cc[2] + ((cz % c.cc[2] + c.cc[2]) % c.cc[2]);
+    const int t = (int)p.w;
+    if (t >= 2 && t < 4) id += c.tot;
+    keys[i] = id;
+    slot[i] = atomicAdd(&counts[id], 1);
+}
+
+// Exclusive scan of counts[0..m) into out[0..m] (out[m] = total), one block:
+// each thread scans a contiguous chunk; chunk totals are scanned in shared memory.
+__global__ void __launch_bounds__(1024) k_mix_scan(const int* __restrict__ counts, int m, int* __restrict__ out) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int chunk = (m + blockDim.x - 1) / blockDim.x;
+    const int b = min(m, t * chunk), e = min(m, b + chunk);
+    int s = 0;
+    for (int k = b; k < e; ++k) s += counts[k];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {  // Hillis-Steele inclusive scan
+        const int v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int run = part[t] - s;
+    for (int k = b; k < e; ++k) {
+        out[k] = run;
+        run += counts[k];
+    }
+    if (t == blockDim.x - 1) out[m] = part[t];
+}
+
+__global__ void k_mix_place(int n, const int* __restrict__ keys, const int* __restrict__ slot,
+                            const int* __restrict__ start, int* __restrict__ tmp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    tmp[start[keys[i]] + slot[i]] = i;
+}
+
+// Order each cell's particles by their previous index (a stable sort overall).
+__global__ void k_mix_rank(int n, const int* __restrict__ keys, const int* __restrict__ start,
+                           const int* __restrict__ tmp, int* __restrict__ perm, int* __restrict__ sorted_keys) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int i = tmp[p];
+    const int key = keys[i];
+    const int b = start[key], e = start[key + 1];
+    int rank = 0;
+    for (int q = b; q < e; ++q) rank += tmp[q] < i;
+    perm[b + rank] = i;
+    sorted_keys[b + rank] = key;
+}
+
+// ---- list build -------------------------------------------------------------
+
+// Home cell and FP32 positions after a sort (sorted order).
+__global__ void k_mix_home(SimConst c, MixConst m, const double4* __restrict__ pos, const int* __restrict__ keys,
+                           const double4* __restrict__ vel, int* __restrict__ home, float4* __restrict__ p32,
+                           float4* __restrict__ p32lo, float4* __restrict__ v32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    int k = keys[i];
+    if (k >= c.tot) k -= c.tot;
+    const int h = pack_cell(k / (c.cc[1] * c.cc[2]), (k / c.cc[2]) % c.cc[1], k % c.cc[2]);
+    home[i] = h;
+    float4 hi, lo;
+    rel32(c, m, pos[i], h, hi, lo);
+    p32[i] = hi;
+    p32lo[i] = lo;
+    const double4 v = vel[i];
+    v32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.0f);
+}
+
+// Neighbour table: for particle i, the 3^D stencil (same visiting order as
+// main.cpp:1356-1392), entries (j << 5 | code); pass 0 keeps pairs within
+// RP+margin, pass 1 the rest within MaxRadius+margin.  Self is excluded.
+// Walls without a fluid neighbour get no list (their pressure is never used).
+__global__ void __launch_bounds__(128)
+k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __restrict__ keys,
+           const int* __restrict__ cellstart, unsigned* __restrict__ list, int cap, int* __restrict__ cnt_short,
+           int* __restrict__ cnt_all, StepScalars* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    int ci = keys[i];
+    if (ci >= c.tot) ci -= c.tot;
+    const int ic[3] = {ci / (c.cc[1] * c.cc[2]), (ci / c.cc[2]) % c.cc[1], ci % c.cc[2]};
+    int jc[3][3], jmin[3], w[3];
+    for (int d = 0; d < 3; ++d) {
+        const int r = c.range[d];
+        w[d] = 2 * r + 1;
+        for (int j = 0; j < w[d]; ++j) jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
+        const int b = (2 * r) - (ic[d] + r) % c.cc[d];
+        jmin[d] = b > 0 ? b : 0;
+    }
+    const float4 pi = p32[i];
+    const int nf = cellstart[c.tot];
+    const bool is_wall = i >= nf;
+    const size_t n = (size_t)c.n;
+    int cnt = 0, cshort = 0;
+    bool any_fluid = !is_wall;  // a wall needs a list only if a fluid particle is within reach
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                    const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
+                    const int cell = jc[0][ax] * c.cc[1] * c.cc[2] + jc[1][ay] * c.cc[2] + jc[2][az];
+                    const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
+                    const float ox = m.dhi[code][0], oy = m.dhi[code][1], oz = m.dhi[code][2];
+                    for (int kind = 0; kind < 2; ++kind) {
+                        const int off = kind ? c.tot : 0;
+                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                        for (int j = b; j < e; ++j) {
+                            if (j == i) continue;
+                            const float4 pj = p32[j];
+                            const float dx = (pj.x - pi.x) + ox, dy = (pj.y - pi.y) + oy, dz = (pj.z - pi.z) + oz;
+                            const float r2 = dx * dx + dy * dy + dz * dz;
+                            const bool near = r2 < m.short_r2;
+                            if (r2 < m.list_r2 && (pass == 0 ? near : !near)) {
+                                if (kind == 0) any_fluid = true;
+                                if (cnt < cap) list[(size_t)cnt * n + i] = ((unsigned)j << kCodeBits) | (unsigned)code;
+                                ++cnt;
+                            }
+                        }
+                    }
+                }
+        if (pass == 0) cshort = cnt;
+    }
+    if (is_wall && !any_fluid) cnt = cshort = 0;
+    cnt_short[i] = cshort;
+    cnt_all[i] = cnt;
+    atomicMax(&scal->max_neighbors, cnt);
+    if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+}
+
+// ---- per step -----------------------------------------------------------------
+
+// Convection, wall motion, periodic wrap and the displacement maximum (the
+// same FP64 expressions as the FP64 form's move), plus the FP32 copies of
+// position (home-relative, hi/lo) and velocity for the pair sweeps.
+__global__ void __launch_bounds__(256)
+k_mix_move(SimConst c, MixConst m, const int* __restrict__ cellstart, double4* __restrict__ pos,
+           double4* __restrict__ vel, const double4* __restrict__ snap, const double* __restrict__ wall_center,
+           const int* __restrict__ home, float4* __restrict__ p32, float4* __restrict__ p32lo,
+           float4* __restrict__ v32, StepScalars* __restrict__ scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s2 = 0.0;
+    if (i < c.n) {
+        const int nf = cellstart[c.tot], we = cellstart[2 * c.tot];
+        double4 p = pos[i];
+        double4 v = vel[i];
+        if (i < nf) {
+            p.x += v.x * c.dt;
+            p.y += v.y * c.dt;
+            p.z += v.z * c.dt;
+        } else if (i < we) {
+            const int t = (int)p.w;
+            const double* C = wall_center + 3 * t;
+            const double(*R)[3] = c.wall_rot[t];
+            const double* W = c.wall_omega[t];
+            const double* U = c.wall_velocity[t];
+            double r0 = p.x - C[0], r1 = p.y - C[1], r2 = p.z - C[2];
+            r0 = R[0][0] * r0 + R[0][1] * r1 + R[0][2] * r2;
+            r1 = R[1][0] * r0 + R[1][1] * r1 + R[1][2] * r2;
+            r2 = R[2][0] * r0 + R[2][1] * r1 + R[2][2] * r2;
+            v.x = W[1] * r2 - W[2] * r1 + U[0];
+            v.y = W[2] * r0 - W[0] * r2 + U[1];
+            v.z = W[0] * r1 - W[1] * r0 + U[2];
+            vel[i] = v;
+            p.x = r0 + C[0] + U[0] * c.dt;
+            p.y = r1 + C[1] + U[1] * c.dt;
+            p.z = r2 + C[2] + U[2] * c.dt;
+        }
+        p.x = omod_fast(p.x - c.dmin[0], c.width[0]) + c.dmin[0];
+        p.y = omod_fast(p.y - c.dmin[1], c.width[1]) + c.dmin[1];
+        p.z = omod_fast(p.z - c.dmin[2], c.width[2]) + c.dmin[2];
+        pos[i] = p;
+        float4 hi, lo;
+        rel32(c, m, p, home[i], hi, lo);
+        p32[i] = hi;
+        p32lo[i] = lo;
+        v32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.0f);
+        const double4 q = snap[i];
+        const double d0 = omod_fast(p.x - q.x + c.half_width[0], c.width[0]) - c.half_width[0];
+        const double d1 = omod_fast(p.y - q.y + c.half_width[1], c.width[1]) - c.half_width[1];
+        const double d2 = omod_fast(p.z - q.z + c.half_width[2], c.width[2]) - c.half_width[2];
+        s2 = d0 * d0 + d1 * d1 + d2 * d2;
+        if (!(s2 > 0.0)) s2 = 0.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, s2, o);
+        s2 = t > s2 ? t : s2;
+    }
+    __shared__ double red[8];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = red[w] > mx ? red[w] : mx;
+        if (mx > 0.0) atomicMax(&scal->max_shift2_bits, (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+// Offset tables in shared memory: per-lane codes differ, and shared memory
+// serves divergent addresses in one access where the constant bank serialises.
+struct SharedTables {
+    float4 dhi[27];
+    float4 dlo[27];
+    float mu[MPH_TYPE_COUNT * MPH_TYPE_COUNT];
+};
+
+__device__ __forceinline__ void load_tables(const MixConst& m, SharedTables& t) {
+    for (int k = threadIdx.x; k < 27; k += blockDim.x) {
+        t.dhi[k] = make_float4(m.dhi[k][0], m.dhi[k][1], m.dhi[k][2], 0.f);
+        t.dlo[k] = make_float4(m.dlo[k][0], m.dlo[k][1], m.dlo[k][2], 0.f);
+    }
+    for (int k = threadIdx.x; k < 16; k += blockDim.x) t.mu[k] = m.visc_mu[k / 4][k % 4];
+    __syncthreads();
+}
+
+// 1/sqrt(r2) with one Newton step (rsqrtf is within 2 ulp; the step brings it
+// to about 1 ulp), for the pressure terms.
+__device__ __forceinline__ float rsqrt_nr(float r2) {
+    const float y = rsqrtf(r2);
+    return y * fmaf(-0.5f * r2 * y, y, 1.5f);
+}
+
+// Surface-tension sums of sweep A for one pair: DensityA and GravityCenter.
+template <bool RATIO>
+__device__ __forceinline__ void st_density(const MixConst& m, int ti, int tj, float r2, float r, float dx, float dy,
+                                           float dz, float& sa, float& cak, float& g0, float& g1, float& g2) {
+    const float ratio = RATIO ? m.ratio[ti][tj] : 1.0f;
+    if (r2 <= m.ra2) {
+        const float q = r * m.inv_ra;
+        kahan_add(sa, cak, ratio * m.ca * q * (1.0f - q) * (1.0f - q));
+    }
+    if (r2 <= m.rg2) {
+        const float q = 1.0f - r * m.inv_rg;
+        const float wgt = ratio * m.cg * q * q * m.inv_r2g_rg;
+        g0 += dx * wgt;
+        g1 += dy * wgt;
+        g2 += dz * wgt;
+    }
+}
+
+// FP64 minimum-image displacement and 1/r from an FP32 seed plus one Newton
+// step (relative error ~1e-14), for the FP64 pressure core.
+__device__ __forceinline__ void disp64(const SimConst& c, const double4& pi, const double4& pj, double& dx, double& dy,
+                                       double& dz) {
+    dx = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+    dy = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+    dz = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+}
+__device__ __forceinline__ double rsqrt64(double r2) {
+    const double y = (double)rsqrtf((float)r2);
+    return y * (1.5 - 0.5 * r2 * y * y);
+}
+
+// Sweep A: DensityP and DivergenceP over the short part of the list with the
+// exact FP32 displacement (S64: in FP64 from the FP64 positions), plus, with
+// surface tension, DensityA and GravityCenter over all of it; epilogue:
+// coefficients, PressureP, PressureA (main.cpp:1631-1662, 1735-1740, 1831-1906).
+template <bool ST, bool RATIO, bool S64>
+__global__ void __launch_bounds__(128)
+k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p32lo, const float4* __restrict__ v32,
+        const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
+        float4* __restrict__ v32p, float4* __restrict__ gca, double* __restrict__ strain_out,
+        double* __restrict__ div_out, double* __restrict__ dens_a_out, double* __restrict__ wall_center,
+        const SimConst c, const double4* __restrict__ pos64, const double4* __restrict__ vel64,
+        double4* __restrict__ press64) {
+    __shared__ SharedTables tb;
+    load_tables(m, tb);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wall_center != nullptr && blockIdx.x == 0 && threadIdx.x < 12) {
+        const int t = threadIdx.x / 3, d = threadIdx.x % 3;
+        if (t >= 2) wall_center[3 * t + d] += c.wall_velocity[t][d] * c.dt;
+    }
+    if (i >= m.n) return;
+    const float4 pi = p32[i];
+    const float4 li = p32lo[i];
+    const float4 vi = v32[i];
+    double4 pid = make_double4(0, 0, 0, 0), vid = make_double4(0, 0, 0, 0);
+    if (S64) {
+        pid = pos64[i];
+        vid = vel64[i];
+    }
+    const int ti = __float_as_int(pi.w);
+    const int ns = cnt_short[i];
+    const int na = ST ? cnt_all[i] : ns;
+    const size_t n = (size_t)m.n;
+    float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
+    double spd = 0.0, sdd = 0.0;
+    float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    const unsigned* lp = list + i;
+    int k = 0;
+    for (; k < ns; ++k, lp += n) {
+        const unsigned e = __ldg(lp);
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = p32[j];
+        const float4 dh = tb.dhi[code];
+        float dx, dy, dz;
+        if (S64) {
+            double dxd, dyd, dzd;
+            disp64(c, pid, pos64[j], dxd, dyd, dzd);
+            const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
+            if (r2d <= c.rp2) {
+                const double y = rsqrt64(r2d);
+                const double q = 1.0 - r2d * y * m.inv_rp_d;
+                spd += m.cp_d * q * q;
+                const double dw = m.cp_m2_d * q;
+                const double4 vj = vel64[j];
+                sdd -= ((vj.x - vid.x) * dxd + (vj.y - vid.y) * dyd + (vj.z - vid.z) * dzd) * y * dw;
+            }
+            dx = (float)dxd;
+            dy = (float)dyd;
+            dz = (float)dzd;
+        } else {
+            const float4 lj = p32lo[j];
+            const float4 dl = tb.dlo[code];
+            dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
+            dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
+            dz = ((pj.z - pi.z) + dh.z) + ((lj.z - li.z) + dl.z);
+        }
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float rinv = rsqrt_nr(r2);
+        const float r = r2 * rinv;
+        if (!S64 && r2 <= m.rp2) {
+            const float q = 1.0f - r * m.inv_rp;
+            kahan_add(sp, cpk, m.cp * q * q);                   // wp
+            const float dw = m.cp_m2 * q;                        // dwpdr
+            const float4 vj = v32[j];
+            const float ue = ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz) * rinv;
+            kahan_add(sd, cdk, -ue * dw);
+        }
+        if (ST) st_density<RATIO>(m, ti, __float_as_int(pj.w), r2, r, dx, dy, dz, sa, cak, g0, g1, g2);
+    }
+    for (; k < na; ++k, lp += n) {  // surface tension only: the long part
+        const unsigned e = __ldg(lp);
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = p32[j];
+        const float4 dh = tb.dhi[code];
+        const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        st_density<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rsqrtf(r2), dx, dy, dz, sa, cak, g0, g1, g2);
+    }
+    double strain, div;
+    if (S64) {
+        strain = spd - m.n0p_d;
+        div = sdd;
+    } else {
+        strain = (double)((sp - cpk) - m.n0p);
+        div = (double)(sd - cdk);
+    }
+    double kappa = c.bulk_modulus[ti];
+    if (strain < 0.0) kappa = 0.0;
+    const double pp = -c.bulk_viscosity[ti] * div + kappa * strain;
+    float pa = 0.0f;
+    if (ST) {
+        const float dens = sa - cak;
+        pa = m.cof_a[ti] * (dens - m.n0a) / m.l0;
+        if (m.n0a <= dens) pa = 0.0f;
+        dens_a_out[i] = dens;
+        gca[i] = make_float4(g0, g1, g2, pa);
+    }
+    v32p[i] = make_float4(vi.x, vi.y, vi.z, (float)pp);
+    if (S64) press64[i] = make_double4(vid.x, vid.y, vid.z, pp);
+    strain_out[i] = strain;
+    div_out[i] = div;
+}
+
+// Surface-tension terms of one pair (PressureA, DiffuseInterface with aj the
+// a of i as the reference has it, main.cpp:1742-1828); returns the radial
+// part and adds the tangential part to t.
+template <bool RATIO>
+__device__ __forceinline__ float st_terms(const MixConst& m, int ti, int tj, float r2, float r, float rinv, float dx,
+                                          float dy, float dz, const float4& gi, const float4& gj, float ai,
+                                          float3& t) {
+    const float rij = RATIO ? m.ratio[ti][tj] : 1.0f, rji = RATIO ? m.ratio[tj][ti] : 1.0f;
+    float s = 0.0f;
+    if (r2 < m.ra2) {
+        const float q = r * m.inv_ra;
+        const float dwa = m.ca_inv * (1.0f - q) * (1.0f - 3.0f * q);
+        s += (gi.w * rij * dwa + gj.w * rji * dwa) * rinv * m.vol;
+    }
+    if (r2 < m.rg2) {
+        const float q = 1.0f - r * m.inv_rg;
+        const float wg = m.cg * q * q, dwg = m.cg_m2 * q;
+        const float k1 = m.inv_r2g_rg * m.vol_over_l0;
+        t.x -= (ai * gj.x * rji * wg - ai * gi.x * rij * wg) * k1;
+        t.y -= (ai * gj.y * rji * wg - ai * gi.y * rij * wg) * k1;
+        t.z -= (ai * gj.z * rji * wg - ai * gi.z * rij * wg) * k1;
+        const float gr = (ai * gj.x * rji * dwg - ai * gi.x * rij * dwg) * dx +
+                         (ai * gj.y * rji * dwg - ai * gi.y * rij * dwg) * dy +
+                         (ai * gj.z * rji * dwg - ai * gi.z * rij * dwg) * dz;
+        s -= gr * rinv * k1;
+    }
+    return s;
+}
+
+// Sweep B for fluid particles (WALLS: for the wall particles, output only).
+// Short part of the list: exact displacement, PressureP + ViscosityV (+ the
+// surface-tension terms), Kahan sums.  Long part: the hi displacement,
+// ViscosityV (+ surface tension), plain FP32 sum.  Then gravity and the FP64
+// velocity update (main.cpp:1908-2010).
+template <bool ST, bool RATIO, bool WALLS, bool S64>
+__global__ void __launch_bounds__(128)
+k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ p32,
+        const float4* __restrict__ p32lo, const float4* __restrict__ v32p, const float4* __restrict__ gca,
+        const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
+        const double4* __restrict__ vel, double4* __restrict__ vel_out, double4* __restrict__ force,
+        StepScalars* __restrict__ scal, const double4* __restrict__ pos64, const double4* __restrict__ press64) {
+    __shared__ SharedTables tb;
+    load_tables(m, tb);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    const int nf = cellstart[c.tot];
+    if (WALLS ? i < nf : i >= nf) {
+        if (!WALLS) vel_out[i] = vel[i];
+        return;
+    }
+    const float4 pi = p32[i];
+    const float4 li = p32lo[i];
+    const float4 vi = v32p[i];
+    const int ti = __float_as_int(pi.w);
+    float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ST) gi = gca[i];
+    const float ai = m.a_k[ti];
+    const int ns = cnt_short[i], na = cnt_all[i];
+    const size_t n = (size_t)m.n;
+    const float mu_u = tb.mu[ti * 4 + ti];
+    float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // short part, Kahan
+    float gx = 0.f, gy = 0.f, gz = 0.f;                                 // long part
+    double hx = 0.0, hy = 0.0, hz = 0.0;                                // short part, FP64 core
+    const unsigned* lp = list + i;
+    int k = 0;
+    if (S64) {
+        const double4 pid = pos64[i];
+        const double4 vid = press64[i];  // {v, PressureP}
+        const double mu_d = c.visc_mu[ti][ti];
+        for (; k < ns; ++k, lp += n) {
+            const unsigned e = __ldg(lp);
+            const int j = (int)(e >> kCodeBits);
+            double dx, dy, dz;
+            disp64(c, pid, pos64[j], dx, dy, dz);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (!(r2 < c.rv2 || r2 < c.rp2 || (ST && (r2 < c.ra2 || r2 < c.rg2)))) continue;
+            const double y = rsqrt64(r2);
+            const double r = r2 * y;
+            const double4 vj = press64[j];
+            const int tj = c.ratio_all_one && m.uniform_mu ? ti : __float_as_int(p32[j].w);
+            double sdd = 0.0;
+            if (r2 < c.rp2) sdd += (vid.w + vj.w) * (m.p_a_d + m.p_b_d * r) * y;
+            if (r2 < c.rv2) {
+                const double mu = m.uniform_mu ? mu_d : c.visc_mu[ti][tj];
+                const double ud = (vj.x - vid.x) * dx + (vj.y - vid.y) * dy + (vj.z - vid.z) * dz;
+                sdd += mu * ud * (m.v_a_d + m.v_b_d * r) * (y * y * y);
+            }
+            if (ST) {
+                float3 t = make_float3(0.f, 0.f, 0.f);
+                const float sf = st_terms<RATIO>(m, ti, tj, (float)r2, (float)r, (float)y, (float)dx, (float)dy,
+                                                 (float)dz, gi, gca[j], ai, t);
+                sdd += sf;
+                hx += t.x;
+                hy += t.y;
+                hz += t.z;
+            }
+            hx += sdd * dx;
+            hy += sdd * dy;
+            hz += sdd * dz;
+        }
+    }
+    for (; k < ns; ++k, lp += n) {
+        const unsigned e = __ldg(lp);
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = p32[j];
+        const float4 lj = p32lo[j];
+        const float4 dh = tb.dhi[code], dl = tb.dlo[code];
+        const float dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
+        const float dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
+        const float dz = ((pj.z - pi.z) + dh.z) + ((lj.z - li.z) + dl.z);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < m.rv2 || r2 < m.rp2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) continue;
+        const float rinv = rsqrt_nr(r2);
+        const float r = r2 * rinv;
+        const int tj = __float_as_int(pj.w);
+        const float4 vj = v32p[j];
+        float s = 0.0f;
+        if (r2 < m.rp2) s += (vi.w + vj.w) * fmaf(m.p_b, r, m.p_a) * rinv;
+        if (r2 < m.rv2) {
+            const float mu = m.uniform_mu ? mu_u : tb.mu[ti * 4 + tj];
+            const float ud = (vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz;
+            s += mu * ud * fmaf(m.v_b, r, m.v_a) * (rinv * rinv * rinv);
+        }
+        float3 t = make_float3(0.f, 0.f, 0.f);
+        if (ST) s += st_terms<RATIO>(m, ti, tj, r2, r, rinv, dx, dy, dz, gi, gca[j], ai, t);
+        kahan_add(fx, cx, fmaf(s, dx, t.x));
+        kahan_add(fy, cy, fmaf(s, dy, t.y));
+        kahan_add(fz, cz, fmaf(s, dz, t.z));
+    }
+    for (; k < na; ++k, lp += n) {
+        const unsigned e = __ldg(lp);
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = p32[j];
+        const float4 dh = tb.dhi[code];
+        const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < m.rv2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) continue;
+        const float rinv = rsqrtf(r2);
+        const float4 vj = v32p[j];
+        float s = 0.0f;
+        if (r2 < m.rv2) {
+            const float r = r2 * rinv;
+            const float mu = m.uniform_mu ? mu_u : tb.mu[ti * 4 + __float_as_int(pj.w)];
+            const float ud = (vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz;
+            s = mu * ud * fmaf(m.v_b, r, m.v_a) * (rinv * rinv * rinv);
+        }
+        float3 t = make_float3(0.f, 0.f, 0.f);
+        if (ST) s += st_terms<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rinv, rinv, dx, dy, dz, gi, gca[j], ai, t);
+        gx = fmaf(s, dx, gx + t.x);
+        gy = fmaf(s, dy, gy + t.y);
+        gz = fmaf(s, dz, gz + t.z);
+    }
+    double F0 = (((double)fx - (double)cx) + hx) + (double)gx;
+    double F1 = (((double)fy - (double)cy) + hy) + (double)gy;
+    double F2 = (((double)fz - (double)cz) + hz) + (double)gz;
+    if (WALLS) {
+        force[i] = make_double4(F0, F1, F2, 0.0);
+        return;
+    }
+    double4 v = vel[i];
+    const double mass = c.density[ti] * c.vol;
+    F0 += mass * c.gravity[0];
+    F1 += mass * c.gravity[1];
+    F2 += mass * c.gravity[2];
+    v.x += F0 / mass * c.dt;
+    v.y += F1 / mass * c.dt;
+    v.z += F2 / mass * c.dt;
+    if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
+    force[i] = make_double4(F0, F1, F2, 0.0);
+    vel_out[i] = v;
+}
+
+// DensityA over the whole list (output only, without surface tension).
+__global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, const unsigned* __restrict__ list,
+                                const int* __restrict__ cnt_all, double* __restrict__ dens_a_out) {
+    __shared__ SharedTables tb;
+    load_tables(m, tb);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    const float4 pi = p32[i];
+    const int ti = __float_as_int(pi.w);
+    const size_t n = (size_t)m.n;
+    float sa = 0.f, ck = 0.f;
+    const unsigned* lp = list + i;
+    for (int k = 0; k < cnt_all[i]; ++k, lp += n) {
+        const unsigned e = *lp;
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = p32[j];
+        const float4 dh = tb.dhi[code];
+        const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= m.ra2) {
+            const float r = sqrtf(r2);
+            const float q = r * m.inv_ra;
+            const float ratio = m.ratio_all_one ? 1.0f : m.ratio[ti][__float_as_int(pj.w)];
+            kahan_add(sa, ck, ratio * m.ca * q * (1.0f - q) * (1.0f - q));
+        }
+    }
+    dens_a_out[i] = sa - ck;
+}
+
+// NeighborCount for output: the list counts plus self (the reference lists
+// self), except walls without a fluid neighbour, whose list is empty there
+// (main.cpp:1416).
+__global__ void k_mix_counts(int n, const int* __restrict__ cnt_all, const int* __restrict__ cellstart, int tot,
+                             int* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = cnt_all[i];
+    out[i] = c > 0 ? c + 1 : (i < cellstart[tot] ? 1 : 0);
+}
+
+inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+struct MixedState {
+    MixConst mc;
+    int* keys_unsorted = nullptr;
+    int* slot = nullptr;
+    int* counts = nullptr;
+    int* tmp = nullptr;
+    int* home = nullptr;
+    float4* p32 = nullptr;
+    float4* p32lo = nullptr;
+    float4* v32 = nullptr;
+    float4* v32p = nullptr;
+    float4* gca = nullptr;
+    unsigned* list = nullptr;
+    int cap = 0;
+    int* cnt_short = nullptr;
+    int* cnt_all = nullptr;
+    StepScalars* h_scal = nullptr;
+    int max_neighbors = 0;
+    bool exported = false;
+    bool s64 = false;  // FP64 pressure core (MPH_MODE_MIXED_P64)
+};
+
+static void mfree(MixedState* m) {
+    void* ptrs[] = {m->keys_unsorted, m->slot, m->counts, m->tmp, m->home, m->p32, m->p32lo, m->v32, m->v32p,
+                    m->gca, m->list, m->cnt_short, m->cnt_all};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (m->h_scal) cudaFreeHost(m->h_scal);
+}
+
+#define MTRY(expr)                                                                     \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            if (err) *err = std::string(#expr ": ") + cudaGetErrorString(e_);          \
+            return MPH_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+template <class T>
+static cudaError_t malloc_n(T** p, size_t n) {
+    return cudaMalloc((void**)p, (n ? n : 1) * sizeof(T));
+}
+
+static int grow_list(MixedState* m, int need, int n, std::string* err) {
+    int cap = ((int)(need * 1.15) + 8 + 31) / 32 * 32;
+    if (m->list) cudaFree(m->list);
+    m->list = nullptr;
+    m->cap = 0;
+    MTRY(malloc_n(&m->list, (size_t)cap * (size_t)n));
+    m->cap = cap;
+    return MPH_OK;
+}
+
+// Counting sort by cell, reorder the FP64 state, home cells, list build.
+int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches) {
+    const int n = c.n, nb = 2 * c.tot;
+    const int a = d.cur, b = 1 - d.cur, va = d.vcur, vb = 1 - d.vcur;
+    int nl = 0;
+    MTRY(cudaMemsetAsync(m->counts, 0, sizeof(int) * (size_t)(nb + 1), s));
+    k_mix_cellkey<<<blocks(n, 256), 256, 0, s>>>(c, d.pos[a], m->keys_unsorted, m->slot, m->counts);
+    k_mix_scan<<<1, 1024, 0, s>>>(m->counts, nb, d.cellstart);
+    k_mix_place<<<blocks(n, 256), 256, 0, s>>>(n, m->keys_unsorted, m->slot, d.cellstart, m->tmp);
+    k_mix_rank<<<blocks(n, 256), 256, 0, s>>>(n, m->keys_unsorted, d.cellstart, m->tmp, d.vals, d.keys);
+    launch_reorder(c, d.vals, d.pidx[a], d.type[a], d.pos[a], d.vel[va], d.pidx[b], d.type[b], d.pos[b], d.vel[vb],
+                   d.snap, s);
+    d.cur = b;
+    d.vcur = vb;
+    k_mix_home<<<blocks(n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->p32,
+                                              m->p32lo, m->v32);
+    nl += 6;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        MTRY(cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), s));
+        k_mix_list<<<blocks(n, 128), 128, 0, s>>>(c, m->mc, m->p32, d.keys, d.cellstart, m->list, m->cap,
+                                                  m->cnt_short, m->cnt_all, d.scal);
+        ++nl;
+        MTRY(cudaGetLastError());
+        MTRY(cudaMemcpyAsync(m->h_scal, d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, s));
+        MTRY(cudaStreamSynchronize(s));
+        m->max_neighbors = m->h_scal->max_neighbors;
+        if (m->max_neighbors <= m->cap) break;
+        const int st = grow_list(m, m->max_neighbors, n, err);
+        if (st != MPH_OK) return st;
+    }
+    if (launches) *launches = nl;
+    if (m->max_neighbors > m->cap) {
+        if (err) *err = "mixed neighbour table could not grow";
+        return MPH_ERR_CAPACITY;
+    }
+    MTRY(cudaMemsetAsync(&d.scal->flags, 0, sizeof(int), s));
+    m->exported = false;
+    return MPH_OK;
+}
+
+void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wall, cudaStream_t s) {
+    const int nb = blocks(c.n, 128);
+    double* wc = advance_wall ? d.wall_center : nullptr;
+#define MIX_A(ST, RATIO, S64)                                                                                   \
+    k_mix_a<ST, RATIO, S64><<<nb, 128, 0, s>>>(m->mc, m->p32, m->p32lo, m->v32, m->list, m->cnt_short,          \
+                                               m->cnt_all, m->v32p, m->gca, d.strain_p, d.div_p, d.dens_a, wc, c, \
+                                               d.pos[d.cur], d.vel[d.vcur], d.press)
+#define MIX_A2(ST, RATIO) \
+    if (m->s64) MIX_A(ST, RATIO, true); else MIX_A(ST, RATIO, false)
+    if (m->mc.has_st) {
+        if (m->mc.ratio_all_one) { MIX_A2(true, false); } else { MIX_A2(true, true); }
+    } else {
+        if (m->mc.ratio_all_one) { MIX_A2(false, false); } else { MIX_A2(false, true); }
+    }
+#undef MIX_A2
+#undef MIX_A
+    m->exported = false;
+}
+
+template <bool WALLS>
+static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
+    const int nb = blocks(c.n, 128);
+    double4* vout = WALLS ? nullptr : d.vel[1 - d.vcur];
+#define MIX_B(ST, RATIO, S64)                                                                                 \
+    k_mix_b<ST, RATIO, WALLS, S64><<<nb, 128, 0, s>>>(m->mc, c, d.cellstart, m->p32, m->p32lo, m->v32p, m->gca, \
+                                                      m->list, m->cnt_short, m->cnt_all, d.vel[d.vcur], vout,     \
+                                                      d.force, d.scal, d.pos[d.cur], d.press)
+#define MIX_B2(ST, RATIO) \
+    if (m->s64) MIX_B(ST, RATIO, true); else MIX_B(ST, RATIO, false)
+    if (m->mc.has_st) {
+        if (m->mc.ratio_all_one) { MIX_B2(true, false); } else { MIX_B2(true, true); }
+    } else {
+        if (m->mc.ratio_all_one) { MIX_B2(false, false); } else { MIX_B2(false, true); }
+    }
+#undef MIX_B2
+#undef MIX_B
+}
+
+void mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
+    launch_b<false>(m, c, d, s);
+    m->exported = false;
+}
+
+void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
+    k_mix_move<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap,
+                                                d.wall_center, m->home, m->p32, m->p32lo, m->v32, d.scal);
+    m->exported = false;
+}
+
+int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, DevFP64& d, bool fp64_pressure,
+                 cudaStream_t s, std::string* err) {
     *out = nullptr;
-    if (err) *err = "mixed form not built yet";
-    return MPH_ERR_ARG;
+    if (c.cc[0] > 1024 || c.cc[1] > 1024 || c.cc[2] > 1024) {
+        if (err) *err = "mixed form: at most 1024 cells per axis";
+        return MPH_ERR_GEOMETRY;
+    }
+    if ((long long)c.n >= (1LL << (32 - kCodeBits))) {
+        if (err) *err = "mixed form: too many particles for the packed list";
+        return MPH_ERR_ARG;
+    }
+    MixedState* m = new MixedState();
+    m->s64 = fp64_pressure;
+    MixConst& mc = m->mc;
+    std::memset(&mc, 0, sizeof(mc));
+    mc.n = c.n;
+    mc.tot = c.tot;
+    mc.dim = c.dim;
+    mc.has_st = c.has_st;
+    mc.ratio_all_one = c.ratio_all_one;
+    for (int dd = 0; dd < 3; ++dd) {
+        mc.cc[dd] = c.cc[dd];
+        mc.range[dd] = c.range[dd];
+    }
+    // hi-part grid: a power of two g with 2.2 cell widths below 2^24 g
+    const double cwmax = std::max(c.cell_width[0], std::max(c.cell_width[1], c.cell_width[2]));
+    mc.grid = std::ldexp(1.0, (int)std::ceil(std::log2(2.2 * cwmax)) - 24);
+    mc.inv_grid = 1.0 / mc.grid;
+    for (int code = 0; code < 27; ++code) {
+        const int dc[3] = {code / 9 - 1, (code / 3) % 3 - 1, code % 3 - 1};
+        for (int dd = 0; dd < 3; ++dd) {
+            const double off = dc[dd] * c.cell_width[dd];
+            const double q = std::rint(off * mc.inv_grid) * mc.grid;
+            mc.dhi[code][dd] = (float)q;
+            mc.dlo[code][dd] = (float)(off - q);
+        }
+        mc.dhi[code][3] = mc.dlo[code][3] = 0.0f;
+    }
+    mc.uniform_mu = 1;
+    for (int t = 0; t < MPH_TYPE_COUNT; ++t)
+        for (int u = 0; u < MPH_TYPE_COUNT; ++u)
+            if (c.visc_mu[t][u] != c.visc_mu[0][0]) mc.uniform_mu = 0;
+    const double margin = 0.1 * c.l0;
+    const double rl = k.max_radius + margin, rs = k.radius_p + margin;
+    mc.list_r2 = (float)(rl * rl);
+    mc.short_r2 = (float)(rs * rs);
+    mc.ra2 = (float)c.ra2;
+    mc.rp2 = (float)c.rp2;
+    mc.rv2 = (float)c.rv2;
+    mc.rg2 = (float)c.rg2;
+    mc.inv_ra = (float)(1.0 / c.ra);
+    mc.inv_rp = (float)(1.0 / c.rp);
+    mc.inv_rv = (float)(1.0 / c.rv);
+    mc.inv_rg = (float)(1.0 / c.rg);
+    mc.ca = (float)c.ca;
+    mc.cp = (float)c.cp;
+    mc.cg = (float)c.cg;
+    mc.cv = (float)c.cv;
+    mc.cp_m2 = (float)(c.cp * c.m2_rp);
+    mc.cg_m2 = (float)(c.cg * c.m2_rg);
+    mc.cv_m2 = (float)(c.cv * c.m2_rv);
+    mc.ca_inv = (float)(c.ca * c.inv_ra);
+    mc.p_a = (float)(c.cp * c.m2_rp * c.vol);
+    mc.p_b = (float)(-c.cp * c.m2_rp * c.vol / c.rp);
+    mc.v_a = (float)(-c.cv * c.m2_rv * c.vol);
+    mc.v_b = (float)(c.cv * c.m2_rv * c.vol / c.rv);
+    mc.p_a_d = c.cp * c.m2_rp * c.vol;
+    mc.p_b_d = -c.cp * c.m2_rp * c.vol / c.rp;
+    mc.v_a_d = -c.cv * c.m2_rv * c.vol;
+    mc.v_b_d = c.cv * c.m2_rv * c.vol / c.rv;
+    mc.cp_d = c.cp;
+    mc.cp_m2_d = c.cp * c.m2_rp;
+    mc.inv_rp_d = 1.0 / c.rp;
+    mc.n0p_d = c.n0p;
+    mc.vol = (float)c.vol;
+    mc.vol_over_l0 = (float)c.vol_over_l0;
+    mc.n0a = (float)c.n0a;
+    mc.n0p = (float)c.n0p;
+    mc.inv_r2g_rg = (float)(c.rg / c.r2g);
+    mc.l0 = (float)c.l0;
+    for (int t = 0; t < MPH_TYPE_COUNT; ++t) {
+        mc.a_k[t] = (float)c.a_k[t];
+        mc.cof_a[t] = (float)c.cof_a[t];
+        mc.bulk_modulus[t] = (float)c.bulk_modulus[t];
+        mc.bulk_viscosity[t] = (float)c.bulk_viscosity[t];
+        for (int u = 0; u < MPH_TYPE_COUNT; ++u) {
+            mc.visc_mu[t][u] = (float)c.visc_mu[t][u];
+            mc.ratio[t][u] = (float)c.ratio[t][u];
+        }
+    }
+    const size_t n = (size_t)c.n;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = malloc_n(&m->keys_unsorted, n);
+    if (e == cudaSuccess) e = malloc_n(&m->slot, n);
+    if (e == cudaSuccess) e = malloc_n(&m->counts, 2 * (size_t)c.tot + 1);
+    if (e == cudaSuccess) e = malloc_n(&m->tmp, n);
+    if (e == cudaSuccess) e = malloc_n(&m->home, n);
+    if (e == cudaSuccess) e = malloc_n(&m->p32, n);
+    if (e == cudaSuccess) e = malloc_n(&m->p32lo, n);
+    if (e == cudaSuccess) e = malloc_n(&m->v32, n);
+    if (e == cudaSuccess) e = malloc_n(&m->v32p, n);
+    if (e == cudaSuccess) e = malloc_n(&m->gca, n);
+    if (e == cudaSuccess) e = malloc_n(&m->cnt_short, n);
+    if (e == cudaSuccess) e = malloc_n(&m->cnt_all, n);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&m->h_scal, sizeof(StepScalars));
+    if (e == cudaSuccess) e = cudaMemsetAsync(m->gca, 0, n * sizeof(float4), s);
+    if (e != cudaSuccess) {
+        if (err) *err = std::string("mixed form allocation: ") + cudaGetErrorString(e);
+        mfree(m);
+        delete m;
+        return MPH_ERR_NOMEM;
+    }
+    // initial table: lattice points within the cut-off, with head room
+    const double ratio = rl / c.l0;
+    const int r = (int)ratio + 1, zr = c.dim == 2 ? 0 : r;
+    int lat = 0;
+    for (int x = -r; x <= r; ++x)
+        for (int y = -r; y <= r; ++y)
+            for (int z = -zr; z <= zr; ++z)
+                if (x * x + y * y + z * z <= ratio * ratio) ++lat;
+    int st = grow_list(m, (int)(lat * 1.1) + 8, c.n, err);
+    if (st == MPH_OK) st = mixed_rebuild(m, c, d, s, err, nullptr);
+    if (st == MPH_OK) {
+        mixed_sweep_a(m, c, d, false, s);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            if (err) *err = cudaGetErrorString(e);
+            st = MPH_ERR_CUDA;
+        }
+    }
+    if (st != MPH_OK) {
+        mfree(m);
+        delete m;
+        return st;
+    }
+    *out = m;
+    return MPH_OK;
 }
-int mixed_step(MixedState*, const SimConst&, DevFP64&, int, cudaStream_t, std::string* err) {
-    if (err) *err = "mixed form not built yet";
-    return MPH_ERR_STATE;
+
+int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches) {
+    int nl = 0;
+    if (!m->exported) {
+        if (!m->mc.has_st) {
+            k_mix_density_a<<<blocks(c.n, 128), 128, 0, s>>>(m->mc, m->p32, m->list, m->cnt_all, d.dens_a);
+            ++nl;
+        }
+        launch_b<true>(m, c, d, s);  // wall forces
+        k_mix_counts<<<blocks(c.n, 256), 256, 0, s>>>(c.n, m->cnt_all, d.cellstart, c.tot, d.ncount);
+        nl += 2;
+        MTRY(cudaGetLastError());
+        m->exported = true;
+    }
+    if (launches) *launches = nl;
+    return MPH_OK;
 }
-int mixed_export(MixedState*, const SimConst&, DevFP64&, cudaStream_t, std::string*) { return MPH_OK; }
-int mixed_import(MixedState*, const SimConst&, DevFP64&, cudaStream_t, std::string*) { return MPH_OK; }
-long long mixed_rebuilds(const MixedState* m) { return m ? m->rebuilds : 0; }
-void mixed_destroy(MixedState* m) { delete m; }
+
+int mixed_import(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err) {
+    // positions/velocities changed from the host: refresh the FP32 copies
+    k_mix_home<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->p32,
+                                                m->p32lo, m->v32);
+    MTRY(cudaGetLastError());
+    m->exported = false;
+    return MPH_OK;
+}
+
+void mixed_mark_stale(MixedState* m) { m->exported = false; }
+int mixed_max_neighbors(const MixedState* m) { return m ? m->max_neighbors : 0; }
+int mixed_capacity(const MixedState* m) { return m ? m->cap : 0; }
+
+void mixed_destroy(MixedState* m) {
+    if (!m) return;
+    mfree(m);
+    delete m;
+}
 
 }  // namespace mph

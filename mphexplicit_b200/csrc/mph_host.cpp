@@ -479,14 +479,15 @@ static int create_impl(mph_ctx* ctx, const int* type, const double* xyz, const d
     CUDA_TRY(ctx, cudaMemcpyAsync(d.wall_center, wc, sizeof(wc), cudaMemcpyHostToDevice, st));
     d.cur = 0;
     d.vcur = 0;
-    TRY(grow_list(ctx, initial_capacity(ctx)));
-    if (ctx->mode == MPH_MODE_MIXED) {
-        TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, st, &ctx->err));
-    }
     // start-up: calculateCellParticle, calculateNeighbor, DensityA, GravityCenter,
     // DensityP (main.cpp:358-364)
-    TRY(rebuild_fp64(ctx));
-    sweep_a(ctx, false);
+    if (ctx->mode != MPH_MODE_FP64) {
+        TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, ctx->mode == MPH_MODE_MIXED_P64, st, &ctx->err));
+    } else {
+        TRY(grow_list(ctx, initial_capacity(ctx)));
+        TRY(rebuild_fp64(ctx));
+        sweep_a(ctx, false);
+    }
     CUDA_TRY(ctx, cudaGetLastError());
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     return MPH_OK;
@@ -498,7 +499,8 @@ extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim
     *out = nullptr;
     if (!p || !h || !type || !xyz || !vel) return fail(nullptr, MPH_ERR_ARG, "NULL argument");
     if (dim != 2 && dim != 3) return fail(nullptr, MPH_ERR_ARG, "dim must be 2 or 3");
-    if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED) return fail(nullptr, MPH_ERR_ARG, "unknown mode");
+    if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED && mode != MPH_MODE_MIXED_P64)
+        return fail(nullptr, MPH_ERR_ARG, "unknown mode");
     if (h->particle_count <= 0) return fail(nullptr, MPH_ERR_ARG, "particle_count must be > 0");
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, MPH_ERR_ARG, "Dt must be finite and > 0");
     for (int d = 0; d < 3; ++d)
@@ -570,16 +572,47 @@ static int step_fp64(mph_ctx* ctx, int nsteps) {
     return MPH_OK;
 }
 
+// The mixed form: same step order, its own kernels (k_mixed.cu).
+static int step_mixed(mph_ctx* ctx, int nsteps) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    for (int k = 0; k < nsteps; ++k) {
+        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+        {
+            Launch L(ctx, "mix_move");
+            mph::mixed_move(ctx->mixed, s, d, st);
+        }
+        TRY(read_scalars(ctx));
+        TRY(check_flags(ctx));
+        double ms;
+        std::memcpy(&ms, &ctx->h_scal->max_shift2_bits, sizeof(double));
+        if (ms > s.shift_thr) {
+            Launch L(ctx, "mix_rebuild");
+            const int rc = mph::mixed_rebuild(ctx->mixed, s, d, st, &ctx->err, &L.count);
+            if (rc != MPH_OK) return fail(ctx, rc, ctx->err);
+            ++ctx->rebuilds;
+        }
+        {
+            Launch L(ctx, "mix_sweep_a");
+            mph::mixed_sweep_a(ctx->mixed, s, d, true, st);
+        }
+        {
+            Launch L(ctx, "mix_sweep_b");
+            mph::mixed_sweep_b(ctx->mixed, s, d, st);
+        }
+        d.vcur = 1 - d.vcur;
+        CUDA_TRY(ctx, cudaGetLastError());
+        ctx->time += ctx->p.dt;  // main.cpp:449
+        ++ctx->step;
+    }
+    ctx->virial_valid = false;
+    return MPH_OK;
+}
+
 extern "C" int mph_step(mph_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return fail(ctx, MPH_ERR_ARG, "bad arguments");
-    if (ctx->mode == MPH_MODE_MIXED) {
-        const int st = mph::mixed_step(ctx->mixed, ctx->sc, ctx->d, nsteps, ctx->stream, &ctx->err);
-        if (st != MPH_OK) return st;
-        ctx->time += ctx->p.dt * nsteps;  // Time += Dt per step (main.cpp:449)
-        ctx->step += nsteps;
-        ctx->virial_valid = false;
-        return MPH_OK;
-    }
+    if (ctx->mode != MPH_MODE_FP64) return step_mixed(ctx, nsteps);
     return step_fp64(ctx, nsteps);
 }
 
@@ -592,7 +625,11 @@ extern "C" int mph_synchronize(mph_ctx* ctx) {
 // The mixed form keeps its own particle order between rebuilds; bring the
 // FP64 buffers up to date before any read-back.
 static int sync_state(mph_ctx* ctx) {
-    if (ctx->mode == MPH_MODE_MIXED) TRY(mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err));
+    if (ctx->mode != MPH_MODE_FP64) {
+        Launch L(ctx, "mix_export");
+        const int rc = mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err, &L.count);
+        if (rc != MPH_OK) return fail(ctx, rc, ctx->err);
+    }
     return MPH_OK;
 }
 
@@ -607,8 +644,7 @@ extern "C" int mph_get_info(mph_ctx* ctx, mph_info* info) {
     CUDA_TRY(ctx, cudaMemcpyAsync(&cs[1], ctx->d.cellstart + tot, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaMemcpyAsync(&cs[2], ctx->d.cellstart + 2 * tot, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     std::vector<int> nc(ctx->n);
-    if (ctx->mode == MPH_MODE_FP64)
-        CUDA_TRY(ctx, cudaMemcpyAsync(nc.data(), ctx->d.ncount, nc.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(nc.data(), ctx->d.ncount, nc.size() * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     long long total = 0;
     for (int v : nc) total += v;
@@ -617,10 +653,10 @@ extern "C" int mph_get_info(mph_ctx* ctx, mph_info* info) {
     info->wall_particle_begin = cs[1];
     info->wall_particle_end = cs[2];
     info->neighbor_ind_count = total;
-    info->max_neighbor_count = ctx->max_neighbors;
-    info->neighbor_capacity = ctx->d.cap;
+    info->max_neighbor_count = ctx->mode != MPH_MODE_FP64 ? mph::mixed_max_neighbors(ctx->mixed) : ctx->max_neighbors;
+    info->neighbor_capacity = ctx->mode != MPH_MODE_FP64 ? mph::mixed_capacity(ctx->mixed) : ctx->d.cap;
     info->step = ctx->step;
-    info->rebuild_count = ctx->mode == MPH_MODE_MIXED ? mph::mixed_rebuilds(ctx->mixed) : ctx->rebuilds;
+    info->rebuild_count = ctx->rebuilds;
     info->time = ctx->time;
     info->mode = ctx->mode;
     return MPH_OK;
@@ -682,7 +718,7 @@ extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel)
         Launch L(ctx, "unpack3");
         mph::launch_unpack3(ctx->n, d.staging, d.vel[d.vcur], nullptr, st);
     }
-    if (ctx->mode == MPH_MODE_MIXED) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
+    if (ctx->mode != MPH_MODE_FP64) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
     CUDA_TRY(ctx, cudaGetLastError());
     return MPH_OK;
 }

@@ -121,7 +121,7 @@ def compute_constants(params: N.Params, header: N.GridHeader, dim: int) -> N.Con
     return c
 
 
-_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED}
+_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED, "mixed_p64": N.MODE_MIXED_P64}
 
 
 class Solver:
