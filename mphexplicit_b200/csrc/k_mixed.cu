@@ -27,6 +27,27 @@ namespace {
 
 constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 
+// Resident 128-thread blocks per SM the force-sweep kernels are compiled for
+// (register cap 65536 / (128 * blocks)), and pairs of the long-range loop whose
+// gathers are issued together; set by measurement on the full dam break.  The
+// FP64-core form runs the sweep as a short-range and a long-range kernel, the
+// FP32 form as one fused kernel.
+#ifndef MPH_MIXB_MINB_SHORT
+#define MPH_MIXB_MINB_SHORT 8
+#endif
+#ifndef MPH_MIXB_MINB_LONG
+#define MPH_MIXB_MINB_LONG 8
+#endif
+#ifndef MPH_MIXB_BATCH
+#define MPH_MIXB_BATCH 3
+#endif
+#ifndef MPH_MIXB_MINB_FUSED
+#define MPH_MIXB_MINB_FUSED 8
+#endif
+#ifndef MPH_MIXB_BATCH_FUSED
+#define MPH_MIXB_BATCH_FUSED 4
+#endif
+
 struct MixConst {
     int n, tot, dim, has_st, ratio_all_one, uniform_mu;
     int cc[3], range[3];
@@ -498,12 +519,18 @@ __device__ __forceinline__ float st_terms(const MixConst& m, int ti, int tj, flo
 }
 
 // Sweep B for fluid particles (WALLS: for the wall particles, output only).
-// Short part of the list: exact displacement, PressureP + ViscosityV (+ the
-// surface-tension terms), Kahan sums.  Long part: the hi displacement,
-// ViscosityV (+ surface tension), plain FP32 sum.  Then gravity and the FP64
-// velocity update (main.cpp:1908-2010).
-template <bool ST, bool RATIO, bool WALLS, bool S64>
-__global__ void __launch_bounds__(128)
+// The short part of the list: exact displacement, PressureP + ViscosityV (+ the
+// surface-tension terms), Kahan sums (or the FP64 core).  The long part: the hi
+// displacement, ViscosityV (+ surface tension), plain FP32 sum.  Then gravity
+// and the FP64 velocity update (main.cpp:1908-2010).
+// PART 2 does both in one pass.  PART 0 (short part, stores the partial force)
+// and PART 1 (long part, adds it) are the same sweep as two launches, so each
+// gets its own register budget; the sum order is unchanged:
+// ((short FP32 - compensation) + FP64 core) + long.
+template <bool ST, bool RATIO, bool WALLS, bool S64, int PART>
+__global__ void __launch_bounds__(128, PART == 0   ? MPH_MIXB_MINB_SHORT
+                                       : PART == 1 ? MPH_MIXB_MINB_LONG
+                                                   : MPH_MIXB_MINB_FUSED)
 k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ p32,
         const float4* __restrict__ p32lo, const float4* __restrict__ v32p, const float4* __restrict__ gca,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
@@ -515,7 +542,7 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     if (i >= m.n) return;
     const int nf = cellstart[c.tot];
     if (WALLS ? i < nf : i >= nf) {
-        if (!WALLS) vel_out[i] = vel[i];
+        if (!WALLS && PART != 0) vel_out[i] = vel[i];
         return;
     }
     const float4 pi = p32[i];
@@ -533,7 +560,10 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     double hx = 0.0, hy = 0.0, hz = 0.0;                                // short part, FP64 core
     const unsigned* lp = list + i;
     int k = 0;
-    if (S64) {
+    if (PART == 1) {
+        k = ns;
+        lp += (size_t)ns * n;
+    } else if (S64) {
         const double4 pid = pos64[i];
         const double4 vid = press64[i];  // {v, PressureP}
         const double mu_d = c.visc_mu[ti][ti];
@@ -569,7 +599,7 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
             hz += sdd * dz;
         }
     }
-    for (; k < ns; ++k, lp += n) {
+    if (PART != 1) for (; k < ns; ++k, lp += n) {
         const unsigned e = __ldg(lp);
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         const float4 pj = p32[j];
@@ -597,16 +627,19 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         kahan_add(fy, cy, fmaf(s, dy, t.y));
         kahan_add(fz, cz, fmaf(s, dz, t.z));
     }
-    for (; k < na; ++k, lp += n) {
-        const unsigned e = __ldg(lp);
-        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
-        const float4 pj = p32[j];
+    if (PART == 0) {
+        force[i] = make_double4(((double)fx - (double)cx) + hx, ((double)fy - (double)cy) + hy,
+                                ((double)fz - (double)cz) + hz, 0.0);
+        return;
+    }
+    // long part: MPH_MIXB_BATCH pairs per iteration, their gathers issued
+    // together so a thread keeps 2 * MPH_MIXB_BATCH independent loads in flight
+    auto long_pair = [&](unsigned e, const float4& pj, const float4& vj) {
+        const int code = (int)(e & 31u);
         const float4 dh = tb.dhi[code];
         const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 < m.rv2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) continue;
         const float rinv = rsqrtf(r2);
-        const float4 vj = v32p[j];
         float s = 0.0f;
         if (r2 < m.rv2) {
             const float r = r2 * rinv;
@@ -614,15 +647,50 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
             const float ud = (vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz;
             s = mu * ud * fmaf(m.v_b, r, m.v_a) * (rinv * rinv * rinv);
         }
-        float3 t = make_float3(0.f, 0.f, 0.f);
-        if (ST) s += st_terms<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rinv, rinv, dx, dy, dz, gi, gca[j], ai, t);
-        gx = fmaf(s, dx, gx + t.x);
-        gy = fmaf(s, dy, gy + t.y);
-        gz = fmaf(s, dz, gz + t.z);
+        if (ST) {
+            if (r2 < m.ra2 || r2 < m.rg2) {
+                const int j = (int)(e >> kCodeBits);
+                float3 t = make_float3(0.f, 0.f, 0.f);
+                s += st_terms<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rinv, rinv, dx, dy, dz, gi, gca[j], ai, t);
+                gx += t.x;
+                gy += t.y;
+                gz += t.z;
+            }
+        }
+        gx = fmaf(s, dx, gx);
+        gy = fmaf(s, dy, gy);
+        gz = fmaf(s, dz, gz);
+    };
+    constexpr int U = PART == 2 ? MPH_MIXB_BATCH_FUSED : MPH_MIXB_BATCH;
+    for (; k + U <= na; k += U, lp += U * n) {
+        unsigned e[U];
+        float4 pj[U], vj[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) e[u] = __ldg(lp + (size_t)u * n);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int j = (int)(e[u] >> kCodeBits);
+            pj[u] = p32[j];
+            vj[u] = v32p[j];
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) long_pair(e[u], pj[u], vj[u]);
     }
-    double F0 = (((double)fx - (double)cx) + hx) + (double)gx;
-    double F1 = (((double)fy - (double)cy) + hy) + (double)gy;
-    double F2 = (((double)fz - (double)cz) + hz) + (double)gz;
+    for (; k < na; ++k, lp += n) {
+        const unsigned e = __ldg(lp);
+        const int j = (int)(e >> kCodeBits);
+        long_pair(e, p32[j], v32p[j]);
+    }
+    double4 fs;
+    if (PART == 1) {
+        fs = force[i];
+    } else {
+        fs = make_double4(((double)fx - (double)cx) + hx, ((double)fy - (double)cy) + hy,
+                          ((double)fz - (double)cz) + hz, 0.0);
+    }
+    double F0 = fs.x + (double)gx;
+    double F1 = fs.y + (double)gy;
+    double F2 = fs.z + (double)gz;
     if (WALLS) {
         force[i] = make_double4(F0, F1, F2, 0.0);
         return;
@@ -801,24 +869,30 @@ template <bool WALLS>
 static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     const int nb = blocks(c.n, 128);
     double4* vout = WALLS ? nullptr : d.vel[1 - d.vcur];
-#define MIX_B(ST, RATIO, S64)                                                                                 \
-    k_mix_b<ST, RATIO, WALLS, S64><<<nb, 128, 0, s>>>(m->mc, c, d.cellstart, m->p32, m->p32lo, m->v32p, m->gca, \
-                                                      m->list, m->cnt_short, m->cnt_all, d.vel[d.vcur], vout,     \
-                                                      d.force, d.scal, d.pos[d.cur], d.press)
-#define MIX_B2(ST, RATIO) \
-    if (m->s64) MIX_B(ST, RATIO, true); else MIX_B(ST, RATIO, false)
+#define MIX_B1(ST, RATIO, S64, PART)                                                                        \
+    k_mix_b<ST, RATIO, WALLS, S64, PART><<<nb, 128, 0, s>>>(                                              \
+        m->mc, c, d.cellstart, m->p32, m->p32lo, m->v32p, m->gca, m->list, m->cnt_short, m->cnt_all,     \
+        d.vel[d.vcur], vout, d.force, d.scal, d.pos[d.cur], d.press)
+#define MIX_B2(ST, RATIO)             \
+    if (m->s64) {                     \
+        MIX_B1(ST, RATIO, true, 0);   \
+        MIX_B1(ST, RATIO, true, 1);   \
+    } else {                          \
+        MIX_B1(ST, RATIO, false, 2);  \
+    }
     if (m->mc.has_st) {
         if (m->mc.ratio_all_one) { MIX_B2(true, false); } else { MIX_B2(true, true); }
     } else {
         if (m->mc.ratio_all_one) { MIX_B2(false, false); } else { MIX_B2(false, true); }
     }
 #undef MIX_B2
-#undef MIX_B
+#undef MIX_B1
 }
 
-void mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
+int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     launch_b<false>(m, c, d, s);
     m->exported = false;
+    return m->s64 ? 2 : 1;
 }
 
 void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
@@ -975,7 +1049,7 @@ int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, s
         }
         launch_b<true>(m, c, d, s);  // wall forces
         k_mix_counts<<<blocks(c.n, 256), 256, 0, s>>>(c.n, m->cnt_all, d.cellstart, c.tot, d.ncount);
-        nl += 2;
+        nl += (m->s64 ? 2 : 1) + 1;
         MTRY(cudaGetLastError());
         m->exported = true;
     }

@@ -599,7 +599,7 @@ static int step_mixed(mph_ctx* ctx, int nsteps) {
         }
         {
             Launch L(ctx, "mix_sweep_b");
-            mph::mixed_sweep_b(ctx->mixed, s, d, st);
+            L.count = mph::mixed_sweep_b(ctx->mixed, s, d, st);
         }
         d.vcur = 1 - d.vcur;
         CUDA_TRY(ctx, cudaGetLastError());

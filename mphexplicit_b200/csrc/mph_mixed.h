@@ -21,8 +21,9 @@ void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
 int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);
 // Density sweep (1 launch); advance_wall moves the wall centres one step.
 void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wall, cudaStream_t s);
-// Force sweep + FP64 velocity update into d.vel[1 - d.vcur] (1 launch).
-void mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
+// Force sweep + FP64 velocity update into d.vel[1 - d.vcur]; returns the
+// number of launches (2 with the FP64 pressure core, else 1).
+int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
 // Fill the output-only fields (DensityA, wall forces, neighbour counts).
 int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);
 // Positions/velocities were overwritten in `d` (mph_set_state): refresh.
