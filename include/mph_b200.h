@@ -44,14 +44,24 @@ extern "C" {
  * neighbour list in the reference order, every pair sum in list order, no FMA
  * contraction.  Results are bit-identical to the reference's x86-64 build. */
 #define MPH_MODE_FP64     0
-/* FP32 pair arithmetic on cell-relative coordinates with compensated
- * per-particle sums; FP64 position/velocity integration; counting-sort cell
- * lists rebuilt every step (no stored neighbour list). */
+/* FP32 pair arithmetic on cell-relative coordinates (exact FP32
+ * displacements from hi/lo parts), compensated per-particle sums, FP64
+ * position/velocity integration; its own counting-sort cell list and a
+ * neighbour table with the short-range pairs first, rebuilt on the
+ * reference's displacement criterion. */
 #define MPH_MODE_MIXED    1
 /* The mixed form with its short-range pressure pairs (DensityP, DivergenceP
  * and the PressureP force, ~12% of the pairs) in FP64 and the long-range
  * pairs (viscosity, surface tension) in FP32. */
 #define MPH_MODE_MIXED_P64 2
+/* The FP64 form with the viscosity and surface-tension pair terms
+ * (ViscosityV main.cpp:1941-1985, DiffuseInterface :1778-1829, PressureA
+ * force :1742-1775) replaced by an edge-MLP surrogate (mph_model) evaluated on
+ * the tensor cores.  Every judge_interval steps the plain FP64 step is run
+ * from the same state as the judge; when the relative L2 error of the fluid
+ * forces exceeds the tolerance, that step and the steps up to the next
+ * judgement take the plain step (fallback).  No reference counterpart. */
+#define MPH_MODE_LEARNED  3
 
 /* ---- parameters read from the *.data file (main.cpp:489-539) --------- */
 typedef struct mph_params {
@@ -270,6 +280,70 @@ int mph_check_exact_division(long long n, unsigned long long seed, long long* mi
 int mph_cell_sort_noalloc(const mph_constants* c, const mph_grid_header* h, int n,
                           const double* xyz, const int* type, int* cell_index,
                           int* cell_particle, int* cell_start, void* stream);
+
+/* ---- learned form: edge-MLP surrogate (no reference counterpart) ------
+ * Network: 9 inputs -> 128 -> 128 -> 128 -> 3, SiLU, BF16 weights and
+ * activations, FP32 accumulation, trained and evaluated by the library's own
+ * tcgen05 kernels.  Inputs of edge (i, j): (x_j - x_i)/l0 (3), (v_j - v_i) /
+ * velocity_scale (3), |x_j - x_i|/l0, type_i, type_j.  Output: the pair's
+ * viscous + surface-tension force on i / force_scale.
+ * A sample is MPH_SAMPLE_FLOATS floats: (dx, dy, dz, r)/l0,
+ * (ux, uy, uz, type_i + 4*type_j), (fx, fy, fz, valid) with f the FP64 pair
+ * term in N.  Parameters are the flat FP32 vector W1[128][16], b1[128],
+ * W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16] (W[out][in]; input
+ * columns >= 9 and output rows >= 3 are padding and stay zero). */
+#define MPH_SAMPLE_FLOATS 12
+typedef struct mph_model mph_model;
+typedef struct mph_dataset mph_dataset;
+
+int mph_model_create(unsigned long long seed, mph_model** out);
+void mph_model_destroy(mph_model* m);
+int mph_model_param_count(void);
+int mph_model_get_params(mph_model* m, float* params);
+int mph_model_set_params(mph_model* m, const float* params);
+int mph_model_set_scales(mph_model* m, double velocity_scale, double force_scale);
+int mph_model_get_scales(mph_model* m, double* velocity_scale, double* force_scale);
+/* One forward + backward pass over n host samples: gradient of the mean
+ * squared error of the scaled outputs (grad[param_count]) and the loss. */
+int mph_model_gradient(mph_model* m, const float* samples, long long n, float* grad, double* loss);
+/* Predicted pair forces (N) of n host samples: out[n][4] = (fx, fy, fz, 0). */
+int mph_model_predict(mph_model* m, const float* samples, long long n, float* out);
+/* Set velocity_scale and force_scale to the RMS of the relative-velocity and
+ * target components of the dataset. */
+int mph_model_fit_scales(mph_model* m, mph_dataset* d);
+/* Adam on shuffled mini-batches of `batch` samples for `epochs` passes over
+ * the dataset; *loss gets the mean loss of the last epoch. */
+int mph_model_train(mph_model* m, mph_dataset* d, int epochs, int batch, double lr, unsigned long long seed,
+                    double* loss);
+int mph_model_last_error(mph_model* m, char* buf, int len);
+
+int mph_dataset_create(long long capacity, mph_dataset** out);
+void mph_dataset_destroy(mph_dataset* d);
+long long mph_dataset_size(mph_dataset* d);
+int mph_dataset_append(mph_dataset* d, const float* samples, long long n);
+int mph_dataset_read(mph_dataset* d, long long first, long long n, float* samples);
+/* Append up to max_samples edges of ctx's current state (fluid particle i,
+ * neighbour j within the viscosity radius), drawn at random with the seed,
+ * with their FP64 viscous + surface-tension pair force as target.  ctx must
+ * be an MPH_MODE_FP64 or MPH_MODE_LEARNED context. */
+int mph_collect_samples(mph_ctx* ctx, mph_dataset* d, long long max_samples, unsigned long long seed);
+
+/* Attach a model to an MPH_MODE_LEARNED context (the context keeps a
+ * reference; the model must outlive it) with the judge interval and the
+ * relative force-error tolerance of the fallback. */
+int mph_set_learned(mph_ctx* ctx, mph_model* m, int judge_interval, double tolerance);
+typedef struct mph_learned_info {
+    long long steps;           /* steps taken in MPH_MODE_LEARNED              */
+    long long learned_steps;   /* steps that used the surrogate                */
+    long long judged;          /* judgements (plain step run beside)           */
+    long long fallbacks;       /* judgements over the tolerance               */
+    long long plain_steps;     /* steps taken by the plain step after a fallback */
+    double last_force_error;   /* relative L2 error of the fluid forces        */
+    double max_force_error;
+    double last_term_error;    /* relative L2 error of the replaced terms      */
+    double max_term_error;
+} mph_learned_info;
+int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);
 
 /* Last error message of ctx (or of the calling thread if ctx is NULL). */
 int mph_last_error(mph_ctx* ctx, char* buf, int len);

@@ -25,6 +25,8 @@ MPH_ERR_GEOMETRY = -9
 MODE_FP64 = 0
 MODE_MIXED = 1
 MODE_MIXED_P64 = 2
+MODE_LEARNED = 3
+SAMPLE_FLOATS = 12
 
 _D4 = C.c_double * TYPE_COUNT
 _D44 = (C.c_double * TYPE_COUNT) * TYPE_COUNT
@@ -123,11 +125,20 @@ class KernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_longlong), ("total_ms", C.c_double)]
 
 
+class LearnedInfo(C.Structure):
+    """mph_learned_info: counters of the learned form."""
+
+    _fields_ = [("steps", C.c_longlong), ("learned_steps", C.c_longlong), ("judged", C.c_longlong),
+                ("fallbacks", C.c_longlong), ("plain_steps", C.c_longlong), ("last_force_error", C.c_double),
+                ("max_force_error", C.c_double), ("last_term_error", C.c_double), ("max_term_error", C.c_double)]
+
+
 # every symbol the header declares, with its ctypes signature
 _P = C.c_void_p
 _I = C.c_int
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
+_fp = C.POINTER(C.c_float)
 SIGNATURES = {
     "mph_params_defaults": (_I, [C.POINTER(Params)]),
     "mph_read_data_file": (_I, [C.c_char_p, C.POINTER(Params), _ip]),
@@ -156,6 +167,26 @@ SIGNATURES = {
     "mph_profile_read": (_I, [_P, C.POINTER(KernelStat), _I, _ip]),
     "mph_check_exact_division": (_I, [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong), _dp]),
     "mph_cell_sort_noalloc": (_I, [C.POINTER(Constants), C.POINTER(GridHeader), _I, _P, _P, _P, _P, _P, _P]),
+    "mph_model_create": (_I, [C.c_ulonglong, C.POINTER(_P)]),
+    "mph_model_destroy": (None, [_P]),
+    "mph_model_param_count": (_I, []),
+    "mph_model_get_params": (_I, [_P, _fp]),
+    "mph_model_set_params": (_I, [_P, _fp]),
+    "mph_model_set_scales": (_I, [_P, C.c_double, C.c_double]),
+    "mph_model_get_scales": (_I, [_P, _dp, _dp]),
+    "mph_model_gradient": (_I, [_P, _fp, C.c_longlong, _fp, _dp]),
+    "mph_model_predict": (_I, [_P, _fp, C.c_longlong, _fp]),
+    "mph_model_fit_scales": (_I, [_P, _P]),
+    "mph_model_train": (_I, [_P, _P, _I, _I, C.c_double, C.c_ulonglong, _dp]),
+    "mph_model_last_error": (_I, [_P, C.c_char_p, _I]),
+    "mph_dataset_create": (_I, [C.c_longlong, C.POINTER(_P)]),
+    "mph_dataset_destroy": (None, [_P]),
+    "mph_dataset_size": (C.c_longlong, [_P]),
+    "mph_dataset_append": (_I, [_P, _fp, C.c_longlong]),
+    "mph_dataset_read": (_I, [_P, C.c_longlong, C.c_longlong, _fp]),
+    "mph_collect_samples": (_I, [_P, _P, C.c_longlong, C.c_ulonglong]),
+    "mph_set_learned": (_I, [_P, _P, _I, C.c_double]),
+    "mph_learned_stats": (_I, [_P, C.POINTER(LearnedInfo)]),
     "mph_last_error": (_I, [_P, C.c_char_p, _I]),
     "mph_destroy": (None, [_P]),
     "mph_version": (C.c_char_p, []),

@@ -226,12 +226,17 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
 // (1742-1775), DiffuseInterface (1782-1828, aj uses the type of i as in the
 // reference), ViscosityV (1943-1984); Force = 0 + fP + fA + fDI + fV, then
 // Gravity (1988-1998) and Acceleration (2000-2010) for fluid particles.
-template <bool ST, bool RATIO>
+// LRN: the learned form.  The PressureA, DiffuseInterface and ViscosityV pair
+// terms are not evaluated; fluid particle i adds instead the sum of its
+// edge-MLP pair forces eforce[eoff[i] .. eoff[i+1]) (FP32, in edge order),
+// which is also stored in lsum[i].
+template <bool ST, bool RATIO, bool LRN>
 __global__ void __launch_bounds__(128, MPH_SWEEP_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
           const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
           const int* __restrict__ ncount, const int* __restrict__ nlist, double4* __restrict__ force,
-          StepScalars* __restrict__ scal) {
+          StepScalars* __restrict__ scal, const int* __restrict__ eoff, const float4* __restrict__ eforce,
+          float4* __restrict__ lsum) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const double4 pi = pos[i];
@@ -261,9 +266,9 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         // PressureA term adds a signed zero to a sum that starts at +0: the sum
         // stays +0 exactly, so the term is skipped (ST == false).
         const bool in_p = c.rp2 - r2 > 0;
-        const bool in_a = ST && (c.ra2 - r2 > 0);
-        const bool in_g = ST && (c.rg2 - r2 > 0);
-        const bool in_v = c.rv2 - r2 > 0;
+        const bool in_a = !LRN && ST && (c.ra2 - r2 > 0);
+        const bool in_g = !LRN && ST && (c.rg2 - r2 > 0);
+        const bool in_v = !LRN && c.rv2 - r2 > 0;
         if (!(in_p || in_a || in_g || in_v)) continue;
         const int tj = type_of(pj);
         const double r = sqrt(r2);
@@ -324,13 +329,28 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
             fv2 += div_rn(cm * dot * e2 * dw, r, ri) * c.vol;
         }
     }
+    const int nf = cellstart[c.tot];
+    if (LRN) {
+        float l0 = 0.f, l1 = 0.f, l2 = 0.f;
+        if (i < nf) {
+            for (int g = eoff[i], ge = eoff[i + 1]; g < ge; ++g) {
+                const float4 q = eforce[g];
+                l0 += q.x;
+                l1 += q.y;
+                l2 += q.z;
+            }
+        }
+        lsum[i] = make_float4(l0, l1, l2, 0.f);
+        fv0 = l0;
+        fv1 = l1;
+        fv2 = l2;
+    }
     double F0 = 0.0, F1 = 0.0, F2 = 0.0;   // resetForce (main.cpp:1617-1628)
     F0 += fp0; F1 += fp1; F2 += fp2;
     F0 += fa0; F1 += fa1; F2 += fa2;
     F0 += fd0; F1 += fd1; F2 += fd2;
     F0 += fv0; F1 += fv1; F2 += fv2;
     double4 vn = make_double4(vi.x, vi.y, vi.z, 0.0);
-    const int nf = cellstart[c.tot];
     if (i < nf) {
         const double m = c.density[ti] * c.vol;
         F0 += m * c.gravity[0];
@@ -486,6 +506,198 @@ k_conserved(SimConst c, const int* __restrict__ cellstart, const double4* __rest
 
 inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
+// ---- learned form ----------------------------------------------------------
+
+// exclusive prefix of ncount[i], i < nf, within blocks of 1024; block totals to bsum
+__global__ void __launch_bounds__(1024) k_edge_scan1(const int* __restrict__ ncount, int nf, int* __restrict__ eoff,
+                                                     int* __restrict__ bsum) {
+    __shared__ int wsum[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = i < nf ? ncount[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        wsum[lane] = t;
+    }
+    __syncthreads();
+    const int before = (w > 0 ? wsum[w - 1] : 0) + x - v;
+    if (i < nf) eoff[i] = before;
+    if (threadIdx.x == 1023) bsum[blockIdx.x] = before + v;
+}
+
+// exclusive prefix of the block totals (one block, chunks of 1024 with a carry)
+__global__ void __launch_bounds__(1024) k_edge_scan2(int* __restrict__ bsum, int nb) {
+    __shared__ int wsum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < nb; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < nb ? bsum[i] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            wsum[lane] = t;
+        }
+        __syncthreads();
+        const int before = carry + (w > 0 ? wsum[w - 1] : 0) + x - v;
+        if (i < nb) bsum[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void __launch_bounds__(1024) k_edge_scan3(int* __restrict__ eoff, const int* __restrict__ bsum, int nf,
+                                                     int nb) {
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    if (i < nf) eoff[i] += bsum[blockIdx.x];
+    if (i == 0) eoff[nf] = bsum[nb];
+}
+
+__global__ void __launch_bounds__(128) k_edge_fill(const int* __restrict__ ncount, const int* __restrict__ nlist,
+                                                   int n, int nf, const int* __restrict__ eoff, int* __restrict__ ei,
+                                                   int* __restrict__ ej) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nf) return;
+    const int b = eoff[i], cnt = ncount[i];
+    for (int k = 0; k < cnt; ++k) {
+        ei[b + k] = i;
+        ej[b + k] = nlist[(size_t)k * n + i];
+    }
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// One training sample per thread: a random CSR edge (i, j), its inputs and
+// the FP64 PressureA + DiffuseInterface + ViscosityV force of j on i, with the
+// expressions of k_sweep_b (main.cpp:1742-1828, 1941-1985).
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(128)
+k_collect(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ velp,
+          const double4* __restrict__ gcpa, const int* __restrict__ ei, const int* __restrict__ ej, long long ne,
+          long long count, unsigned long long seed, float4* __restrict__ out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    const long long g = (long long)(mix64(seed ^ mix64((unsigned long long)q)) % (unsigned long long)ne);
+    const int i = ei[g], j = ej[g];
+    const double4 pi = pos[i], pj = pos[j];
+    double x[3];
+    disp(c, pi, pj, x);
+    const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+    const bool in_a = ST && (c.ra2 - r2 > 0);
+    const bool in_g = ST && (c.rg2 - r2 > 0);
+    const bool in_v = c.rv2 - r2 > 0;
+    const int ti = type_of(pi), tj = type_of(pj);
+    const double4 vi = velp[i], vj = velp[j];
+    double f0 = 0.0, f1 = 0.0, f2 = 0.0;
+    const bool valid = i != j && (in_a || in_g || in_v);
+    const double r = sqrt(r2);
+    if (valid) {
+        const double ri = __drcp_rn(r);
+        const double e0 = div_rn(x[0], r, ri), e1 = div_rn(x[1], r, ri), e2 = div_rn(x[2], r, ri);
+        const double qa = div_rn(r, c.ra, c.inv_ra);
+        double rij = 1.0, rji = 1.0;
+        if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
+        if (in_a) {
+            const double dwa = s_dwa(c, qa);
+            const double s = gcpa[i].w * (RATIO ? rij * dwa : dwa) + gcpa[j].w * (RATIO ? rji * dwa : dwa);
+            f0 += s * e0 * c.vol;
+            f1 += s * e1 * c.vol;
+            f2 += s * e2 * c.vol;
+        }
+        if (ST && in_g) {
+            const double4 gci = gcpa[i], gcj = gcpa[j];
+            const double ai = c.a_k[ti], aj = ai;
+            const double qg = c.rg_eq_ra ? qa : div_rn(r, c.rg, c.inv_rg);
+            const double wg = s_wg(c, qg);
+            const double wij = RATIO ? rij * wg : wg, wji = RATIO ? rji * wg : wg;
+            f0 -= div_rn(aj * gcj.x * wji - ai * gci.x * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            f1 -= div_rn(aj * gcj.y * wji - ai * gci.y * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            f2 -= div_rn(aj * gcj.z * wji - ai * gci.z * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            const double dg = s_dwg(c, qg);
+            const double dwij = RATIO ? rij * dg : dg, dwji = RATIO ? rji * dg : dg;
+            double gr = 0.0;
+            gr += (aj * gcj.x * dwji - ai * gci.x * dwij) * x[0];
+            gr += (aj * gcj.y * dwji - ai * gci.y * dwij) * x[1];
+            gr += (aj * gcj.z * dwji - ai * gci.z * dwij) * x[2];
+            f0 -= div_rn(gr * e0, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            f1 -= div_rn(gr * e1, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            f2 -= div_rn(gr * e2, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+        }
+        if (in_v) {
+            const double qv = c.rv_eq_ra ? qa : div_rn(r, c.rv, c.inv_rv);
+            const double dw = -s_dwv(c, qv);
+            const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+            const double dot = u0 * e0 + u1 * e1 + u2 * e2;
+            const double cm = c.visc_mu[ti][tj];
+            f0 += div_rn(cm * dot * e0 * dw, r, ri) * c.vol;
+            f1 += div_rn(cm * dot * e1 * dw, r, ri) * c.vol;
+            f2 += div_rn(cm * dot * e2 * dw, r, ri) * c.vol;
+        }
+    }
+    const double il0 = 1.0 / c.l0;
+    out[3 * q + 0] = make_float4((float)(x[0] * il0), (float)(x[1] * il0), (float)(x[2] * il0), (float)(r * il0));
+    out[3 * q + 1] = make_float4((float)(vj.x - vi.x), (float)(vj.y - vi.y), (float)(vj.z - vi.z),
+                                 (float)(ti + 4 * tj));
+    out[3 * q + 2] = make_float4((float)f0, (float)f1, (float)f2, valid ? 1.f : 0.f);
+}
+
+__global__ void __launch_bounds__(256)
+k_force_compare(int nf, const double4* __restrict__ fa, const double4* __restrict__ fb,
+                const float4* __restrict__ lsum, double* __restrict__ sums) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    if (i < nf) {
+        const double4 a = fa[i], b = fb[i];
+        const float4 l = lsum[i];
+        const double d0 = a.x - b.x, d1 = a.y - b.y, d2 = a.z - b.z;
+        s0 = d0 * d0 + d1 * d1 + d2 * d2;
+        s1 = b.x * b.x + b.y * b.y + b.z * b.z;
+        const double v0 = (double)l.x - d0, v1 = (double)l.y - d1, v2 = (double)l.z - d2;
+        s2 = v0 * v0 + v1 * v1 + v2 * v2;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&sums[0], s0);
+        atomicAdd(&sums[1], s1);
+        atomicAdd(&sums[2], s2);
+    }
+}
+
 }  // namespace
 
 void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel, const double4* snap,
@@ -514,19 +726,22 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
                     double4* vel_out, const double4* press, const double4* gc, const int* ncount,
-                    const int* nlist, double4* force, StepScalars* scal, cudaStream_t s) {
+                    const int* nlist, double4* force, StepScalars* scal, cudaStream_t s, const int* eoff,
+                    const float4* eforce, float4* lsum) {
+    (void)vel_in;
     const int nb = blocks(c.n, 128);
+#define SWEEP_B(ST, RATIO, LRN) \
+    k_sweep_b<ST, RATIO, LRN><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal, \
+                                                 eoff, eforce, lsum)
+#define SWEEP_B2(ST, RATIO) \
+    if (eforce) SWEEP_B(ST, RATIO, true); else SWEEP_B(ST, RATIO, false)
     if (c.has_st) {
-        if (c.ratio_all_one)
-            k_sweep_b<true, false><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
-        else
-            k_sweep_b<true, true><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
+        if (c.ratio_all_one) { SWEEP_B2(true, false); } else { SWEEP_B2(true, true); }
     } else {
-        if (c.ratio_all_one)
-            k_sweep_b<false, false><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
-        else
-            k_sweep_b<false, true><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal);
+        if (c.ratio_all_one) { SWEEP_B2(false, false); } else { SWEEP_B2(false, true); }
     }
+#undef SWEEP_B2
+#undef SWEEP_B
 }
 
 void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double4* press,
@@ -543,6 +758,43 @@ int check_division(unsigned long long seed, long long n, unsigned long long* d_c
 void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,
                       double* partial, cudaStream_t s) {
     k_conserved<<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, partial);
+}
+
+int edge_scan_blocks(int nf) { return (nf + 1023) / 1024 + 1; }
+
+void launch_edge_offsets(const int* ncount, int nf, int* eoff, int* bsum, cudaStream_t s) {
+    const int nb = (nf + 1023) / 1024;
+    if (nb == 0) {
+        cudaMemsetAsync(eoff, 0, sizeof(int), s);
+        return;
+    }
+    k_edge_scan1<<<nb, 1024, 0, s>>>(ncount, nf, eoff, bsum);
+    k_edge_scan2<<<1, 1024, 0, s>>>(bsum, nb);
+    k_edge_scan3<<<nb, 1024, 0, s>>>(eoff, bsum, nf, nb);
+}
+
+void launch_edge_fill(const int* ncount, const int* nlist, int n, int nf, const int* eoff, int* ei, int* ej,
+                      cudaStream_t s) {
+    if (nf > 0) k_edge_fill<<<blocks(nf, 128), 128, 0, s>>>(ncount, nlist, n, nf, eoff, ei, ej);
+}
+
+void launch_collect(const SimConst& c, const double4* pos, const double4* press, const double4* gc, const int* ei,
+                    const int* ej, long long ne, long long count, unsigned long long seed, float4* out,
+                    cudaStream_t s) {
+    if (count <= 0 || ne <= 0) return;
+    const unsigned nb = (unsigned)((count + 127) / 128);
+#define COLLECT(ST, RATIO) k_collect<ST, RATIO><<<nb, 128, 0, s>>>(c, pos, press, gc, ei, ej, ne, count, seed, out)
+    if (c.has_st) {
+        if (c.ratio_all_one) COLLECT(true, false); else COLLECT(true, true);
+    } else {
+        if (c.ratio_all_one) COLLECT(false, false); else COLLECT(false, true);
+    }
+#undef COLLECT
+}
+
+void launch_force_compare(int nf, const double4* fa, const double4* fb, const float4* lsum, double* sums3,
+                          cudaStream_t s) {
+    if (nf > 0) k_force_compare<<<blocks(nf, 256), 256, 0, s>>>(nf, fa, fb, lsum, sums3);
 }
 
 }  // namespace mph

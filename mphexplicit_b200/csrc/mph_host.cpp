@@ -20,6 +20,7 @@
 #include "mph_internal.h"
 #include "mph_io.h"
 #include "mph_mixed.h"
+#include "mph_learned.h"
 
 using mph::SimConst;
 using mph::StepScalars;
@@ -39,8 +40,31 @@ struct Profiler {
     std::vector<cudaEvent_t> pool;
 };
 
+// The learned form's device buffers and counters (MPH_MODE_LEARNED).
+struct LearnedState {
+    mph_model* model = nullptr;
+    int judge_interval = 20;
+    double tol = 1e-2;
+    int* eoff = nullptr;        // CSR offsets of the fluid particles' edges [nf + 1]
+    int* bsum = nullptr;        // scan scratch
+    int* ei = nullptr;          // edge -> i
+    int* ej = nullptr;          // edge -> j
+    float4* eforce = nullptr;   // edge-MLP pair forces
+    long long ecap = 0, ne = 0;
+    bool edges_valid = false;
+    float4* lsum = nullptr;     // per-particle learned force
+    double4* force_j = nullptr; // the judge's forces and velocities
+    double4* vel_j = nullptr;
+    double* sums = nullptr;     // device [3]
+    double* h_sums = nullptr;   // pinned [3]
+    int fallback_left = 0;
+    mph_learned_info info{};
+};
+
 struct mph_ctx {
     int mode = MPH_MODE_FP64;
+    int n_fluid = 0;
+    LearnedState lrn;
     int dim = 3;
     int n = 0;
     mph_params p{};
@@ -425,6 +449,7 @@ static int rebuild_fp64(mph_ctx* ctx) {
     if (ctx->max_neighbors > d.cap) return fail(ctx, MPH_ERR_CAPACITY, "neighbour table could not grow");
     // the overflow flag of the attempts that grew the table is not an error
     CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->flags, 0, sizeof(int), st));
+    ctx->lrn.edges_valid = false;
     return MPH_OK;
 }
 
@@ -452,6 +477,19 @@ extern "C" void mph_destroy(mph_ctx* ctx) {
     for (auto& q : ctx->prof.pending) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
     for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
     if (ctx->mixed) mph::mixed_destroy(ctx->mixed);
+    {
+        LearnedState& L = ctx->lrn;
+        cudaFree(L.eoff);
+        cudaFree(L.bsum);
+        cudaFree(L.ei);
+        cudaFree(L.ej);
+        cudaFree(L.eforce);
+        cudaFree(L.lsum);
+        cudaFree(L.force_j);
+        cudaFree(L.vel_j);
+        cudaFree(L.sums);
+        if (L.h_sums) cudaFreeHost(L.h_sums);
+    }
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -481,7 +519,7 @@ static int create_impl(mph_ctx* ctx, const int* type, const double* xyz, const d
     d.vcur = 0;
     // start-up: calculateCellParticle, calculateNeighbor, DensityA, GravityCenter,
     // DensityP (main.cpp:358-364)
-    if (ctx->mode != MPH_MODE_FP64) {
+    if (ctx->mode == MPH_MODE_MIXED || ctx->mode == MPH_MODE_MIXED_P64) {
         TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, ctx->mode == MPH_MODE_MIXED_P64, st, &ctx->err));
     } else {
         TRY(grow_list(ctx, initial_capacity(ctx)));
@@ -499,7 +537,7 @@ extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim
     *out = nullptr;
     if (!p || !h || !type || !xyz || !vel) return fail(nullptr, MPH_ERR_ARG, "NULL argument");
     if (dim != 2 && dim != 3) return fail(nullptr, MPH_ERR_ARG, "dim must be 2 or 3");
-    if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED && mode != MPH_MODE_MIXED_P64)
+    if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED && mode != MPH_MODE_MIXED_P64 && mode != MPH_MODE_LEARNED)
         return fail(nullptr, MPH_ERR_ARG, "unknown mode");
     if (h->particle_count <= 0) return fail(nullptr, MPH_ERR_ARG, "particle_count must be > 0");
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, MPH_ERR_ARG, "Dt must be finite and > 0");
@@ -508,6 +546,7 @@ extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim
     TRY(validate_inputs(h->particle_count, type, xyz, vel));
     mph_ctx* ctx = new mph_ctx();
     ctx->mode = mode;
+    for (int i = 0; i < h->particle_count; ++i) ctx->n_fluid += type[i] < 2 ? 1 : 0;
     ctx->dim = dim;
     ctx->n = h->particle_count;
     ctx->p = *p;
@@ -610,9 +649,202 @@ static int step_mixed(mph_ctx* ctx, int nsteps) {
     return MPH_OK;
 }
 
+// ---- the learned form --------------------------------------------------------
+
+// CSR edges of the fluid particles' neighbour lists (after each rebuild).
+static int build_edges(mph_ctx* ctx) {
+    LearnedState& L = ctx->lrn;
+    mph::DevFP64& d = ctx->d;
+    cudaStream_t st = ctx->stream;
+    const int nf = ctx->n_fluid;
+    if (!L.eoff) {
+        TRY(dalloc(ctx, &L.eoff, (size_t)nf + 1));
+        TRY(dalloc(ctx, &L.bsum, (size_t)mph::edge_scan_blocks(nf) + 1));
+    }
+    {
+        Launch Lc(ctx, "edge_offsets");
+        Lc.count = 3;
+        mph::launch_edge_offsets(d.ncount, nf, L.eoff, L.bsum, st);
+    }
+    int ne = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&ne, L.eoff + nf, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (ne > L.ecap) {
+        cudaFree(L.ei);
+        cudaFree(L.ej);
+        cudaFree(L.eforce);
+        L.ei = L.ej = nullptr;
+        L.eforce = nullptr;
+        L.ecap = 0;
+        const long long cap = (long long)(ne * 1.2) + 1024;
+        TRY(dalloc(ctx, &L.ei, (size_t)cap));
+        TRY(dalloc(ctx, &L.ej, (size_t)cap));
+        if (ctx->mode == MPH_MODE_LEARNED) TRY(dalloc(ctx, &L.eforce, (size_t)cap));
+        L.ecap = cap;
+    }
+    L.ne = ne;
+    {
+        Launch Lc(ctx, "edge_fill");
+        mph::launch_edge_fill(d.ncount, d.nlist, ctx->n, nf, L.eoff, L.ei, L.ej, st);
+    }
+    CUDA_TRY(ctx, cudaGetLastError());
+    L.edges_valid = true;
+    return MPH_OK;
+}
+
+static int learned_buffers(mph_ctx* ctx) {
+    LearnedState& L = ctx->lrn;
+    if (L.lsum) return MPH_OK;
+    const size_t n = (size_t)ctx->n;
+    TRY(dalloc(ctx, &L.lsum, n));
+    TRY(dalloc(ctx, &L.force_j, n));
+    TRY(dalloc(ctx, &L.vel_j, n));
+    TRY(dalloc(ctx, &L.sums, 3));
+    CUDA_TRY(ctx, cudaMallocHost((void**)&L.h_sums, 3 * sizeof(double)));
+    return MPH_OK;
+}
+
+static void plain_sweep_b(mph_ctx* ctx, double4* vel_out, double4* force) {
+    mph::DevFP64& d = ctx->d;
+    Launch L(ctx, "sweep_b");
+    mph::launch_sweep_b(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vel_out, d.press, d.gc, d.ncount, d.nlist,
+                        force, d.scal, ctx->stream);
+}
+
+// The FP64 step with the learned pair terms, the judge and the fallback.
+static int step_learned(mph_ctx* ctx, int nsteps) {
+    LearnedState& L = ctx->lrn;
+    if (!L.model) return fail(ctx, MPH_ERR_STATE, "no model attached (mph_set_learned)");
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    TRY(learned_buffers(ctx));
+    mph::mlp::Model* md = mph::model_of(L.model);
+    for (int k = 0; k < nsteps; ++k) {
+        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+        {
+            Launch Lm(ctx, "move");
+            mph::launch_move(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap, d.wall_center, d.scal, st);
+        }
+        TRY(read_scalars(ctx));
+        TRY(check_flags(ctx));
+        double ms;
+        std::memcpy(&ms, &ctx->h_scal->max_shift2_bits, sizeof(double));
+        if (ms > s.shift_thr) {
+            TRY(rebuild_fp64(ctx));
+            ++ctx->rebuilds;
+        }
+        sweep_a(ctx, true);
+        double4* vout = d.vel[1 - d.vcur];
+        if (L.fallback_left > 0) {
+            plain_sweep_b(ctx, vout, d.force);
+            --L.fallback_left;
+            ++L.info.plain_steps;
+        } else {
+            if (!L.edges_valid) TRY(build_edges(ctx));
+            mph::mlp::EdgeSource es{};
+            es.pos = d.pos[d.cur];
+            es.vel = d.press;
+            es.ei = L.ei;
+            es.ej = L.ej;
+            es.ne = L.ne;
+            for (int q = 0; q < 3; ++q) {
+                es.width[q] = s.width[q];
+                es.half_width[q] = s.half_width[q];
+            }
+            es.inv_l0 = 1.0 / s.l0;
+            es.rv2 = s.rv2;
+            {
+                Launch Lm(ctx, "mlp_edges");
+                if (mph::mlp::model_apply_edges(md, es, L.eforce, st, &Lm.count, &ctx->err) != 0)
+                    return fail(ctx, MPH_ERR_CUDA, ctx->err);
+            }
+            {
+                Launch Lb(ctx, "sweep_b_learned");
+                mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vout, d.press, d.gc, d.ncount,
+                                    d.nlist, d.force, d.scal, st, L.eoff, L.eforce, L.lsum);
+            }
+            bool use = true;
+            if (L.info.steps % L.judge_interval == 0) {
+                plain_sweep_b(ctx, L.vel_j, L.force_j);
+                CUDA_TRY(ctx, cudaMemsetAsync(L.sums, 0, 3 * sizeof(double), st));
+                {
+                    Launch Lc(ctx, "force_compare");
+                    mph::launch_force_compare(ctx->n_fluid, d.force, L.force_j, L.lsum, L.sums, st);
+                }
+                CUDA_TRY(ctx, cudaMemcpyAsync(L.h_sums, L.sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+                CUDA_TRY(ctx, cudaStreamSynchronize(st));
+                std::string merr;
+                if (mph::mlp::model_error_flag(md, &merr) != 0) return fail(ctx, MPH_ERR_DEVICE, merr);
+                const double e = L.h_sums[1] > 0.0 ? std::sqrt(L.h_sums[0] / L.h_sums[1]) : 0.0;
+                const double te = L.h_sums[2] > 0.0 ? std::sqrt(L.h_sums[0] / L.h_sums[2]) : 0.0;
+                ++L.info.judged;
+                L.info.last_force_error = e;
+                L.info.last_term_error = te;
+                L.info.max_force_error = std::max(L.info.max_force_error, e);
+                L.info.max_term_error = std::max(L.info.max_term_error, te);
+                if (!(e <= L.tol)) {  // fall back: take the judge's step
+                    use = false;
+                    ++L.info.fallbacks;
+                    ++L.info.plain_steps;
+                    L.fallback_left = L.judge_interval - 1;
+                    const size_t bytes = (size_t)ctx->n * sizeof(double4);
+                    CUDA_TRY(ctx, cudaMemcpyAsync(vout, L.vel_j, bytes, cudaMemcpyDeviceToDevice, st));
+                    CUDA_TRY(ctx, cudaMemcpyAsync(d.force, L.force_j, bytes, cudaMemcpyDeviceToDevice, st));
+                }
+            }
+            if (use) ++L.info.learned_steps;
+        }
+        ++L.info.steps;
+        d.vcur = 1 - d.vcur;
+        CUDA_TRY(ctx, cudaGetLastError());
+        ctx->time += ctx->p.dt;
+        ++ctx->step;
+    }
+    ctx->virial_valid = false;
+    return MPH_OK;
+}
+
+extern "C" int mph_set_learned(mph_ctx* ctx, mph_model* m, int judge_interval, double tolerance) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    if (ctx->mode != MPH_MODE_LEARNED) return fail(ctx, MPH_ERR_STATE, "the context is not in MPH_MODE_LEARNED");
+    if (!m || judge_interval < 1 || !(tolerance > 0.0)) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    ctx->lrn.model = m;
+    ctx->lrn.judge_interval = judge_interval;
+    ctx->lrn.tol = tolerance;
+    ctx->lrn.fallback_left = 0;
+    return MPH_OK;
+}
+
+extern "C" int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info) {
+    if (!ctx || !info) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    *info = ctx->lrn.info;
+    return MPH_OK;
+}
+
+extern "C" int mph_collect_samples(mph_ctx* ctx, mph_dataset* ds, long long max_samples, unsigned long long seed) {
+    if (!ctx || !ds || max_samples < 0) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "samples come from the FP64 neighbour list (FP64 or learned form)");
+    if (!ctx->lrn.edges_valid) TRY(build_edges(ctx));
+    long long got = 0;
+    float4* dst = mph::dataset_reserve(ds, max_samples, &got);
+    if (got < max_samples) return fail(ctx, MPH_ERR_CAPACITY, "dataset is full");
+    mph::DevFP64& d = ctx->d;
+    {
+        Launch L(ctx, "collect");
+        mph::launch_collect(ctx->sc, d.pos[d.cur], d.press, d.gc, ctx->lrn.ei, ctx->lrn.ej, ctx->lrn.ne, got, seed, dst,
+                            ctx->stream);
+    }
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    mph::dataset_commit(ds, got);
+    return MPH_OK;
+}
+
 extern "C" int mph_step(mph_ctx* ctx, int nsteps) {
     if (!ctx || nsteps < 0) return fail(ctx, MPH_ERR_ARG, "bad arguments");
-    if (ctx->mode != MPH_MODE_FP64) return step_mixed(ctx, nsteps);
+    if (ctx->mixed) return step_mixed(ctx, nsteps);
+    if (ctx->mode == MPH_MODE_LEARNED) return step_learned(ctx, nsteps);
     return step_fp64(ctx, nsteps);
 }
 
@@ -625,7 +857,7 @@ extern "C" int mph_synchronize(mph_ctx* ctx) {
 // The mixed form keeps its own particle order between rebuilds; bring the
 // FP64 buffers up to date before any read-back.
 static int sync_state(mph_ctx* ctx) {
-    if (ctx->mode != MPH_MODE_FP64) {
+    if (ctx->mixed) {
         Launch L(ctx, "mix_export");
         const int rc = mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err, &L.count);
         if (rc != MPH_OK) return fail(ctx, rc, ctx->err);
@@ -653,8 +885,8 @@ extern "C" int mph_get_info(mph_ctx* ctx, mph_info* info) {
     info->wall_particle_begin = cs[1];
     info->wall_particle_end = cs[2];
     info->neighbor_ind_count = total;
-    info->max_neighbor_count = ctx->mode != MPH_MODE_FP64 ? mph::mixed_max_neighbors(ctx->mixed) : ctx->max_neighbors;
-    info->neighbor_capacity = ctx->mode != MPH_MODE_FP64 ? mph::mixed_capacity(ctx->mixed) : ctx->d.cap;
+    info->max_neighbor_count = ctx->mixed ? mph::mixed_max_neighbors(ctx->mixed) : ctx->max_neighbors;
+    info->neighbor_capacity = ctx->mixed ? mph::mixed_capacity(ctx->mixed) : ctx->d.cap;
     info->step = ctx->step;
     info->rebuild_count = ctx->rebuilds;
     info->time = ctx->time;
@@ -718,7 +950,7 @@ extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel)
         Launch L(ctx, "unpack3");
         mph::launch_unpack3(ctx->n, d.staging, d.vel[d.vcur], nullptr, st);
     }
-    if (ctx->mode != MPH_MODE_FP64) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
+    if (ctx->mixed) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
     CUDA_TRY(ctx, cudaGetLastError());
     return MPH_OK;
 }
@@ -747,7 +979,7 @@ extern "C" int mph_get_fields(mph_ctx* ctx, double* divergence_p, double* pressu
 
 extern "C" int mph_get_cells(mph_ctx* ctx, int* cell_index, int* fb, int* fe, int* wb, int* we) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "cell data is kept by the FP64 form only");
+    if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "cell data is kept by the FP64 form only");
     const int tot = ctx->sc.tot;
     std::vector<int> cs(2 * (size_t)tot + 1);
     TRY(d2h(ctx, cell_index, ctx->d.keys, (size_t)ctx->n));
@@ -765,7 +997,7 @@ extern "C" int mph_get_cells(mph_ctx* ctx, int* cell_index, int* fb, int* fe, in
 
 extern "C" int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long long ind_capacity) {
     if (!ctx || !ptr) return fail(ctx, MPH_ERR_ARG, "bad arguments");
-    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "the neighbour list is kept by the FP64 form only");
+    if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "the neighbour list is kept by the FP64 form only");
     const size_t n = (size_t)ctx->n;
     std::vector<int> nc(n);
     CUDA_TRY(ctx, cudaMemcpyAsync(nc.data(), ctx->d.ncount, n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -786,7 +1018,7 @@ extern "C" int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long lo
 
 extern "C" int mph_compute_virial(mph_ctx* ctx) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    if (ctx->mode != MPH_MODE_FP64) return fail(ctx, MPH_ERR_STATE, "virial stress is computed by the FP64 form");
+    if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "virial stress is computed by the FP64 form");
     mph::DevFP64& d = ctx->d;
     {
         Launch L(ctx, "virial");

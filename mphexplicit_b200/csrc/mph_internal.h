@@ -112,10 +112,31 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel, const int* ncount, const int* nlist, int cap_stride,
                     double* dens_a, double* strain_p, double* div_p, double4* press, double4* gc,
                     double* wall_center, cudaStream_t s);
+// eforce != nullptr: the learned form (edge-MLP pair forces replace the
+// PressureA, DiffuseInterface and ViscosityV terms; see k_sweep_b)
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel_in, double4* vel_out, const double4* press,
                     const double4* gc, const int* ncount, const int* nlist, double4* force,
-                    StepScalars* scal, cudaStream_t s);
+                    StepScalars* scal, cudaStream_t s, const int* eoff = nullptr,
+                    const float4* eforce = nullptr, float4* lsum = nullptr);
+
+// ---- learned form (k_fp64.cu) ---------------------------------------------
+// CSR edges of the fluid particles' lists (i < nf): eoff[0..nf] = exclusive
+// prefix of ncount (bsum: scratch of edge_scan_blocks(nf) ints), then
+// ei/ej = (i, list entry) for every edge, self entries included.
+int edge_scan_blocks(int nf);
+void launch_edge_offsets(const int* ncount, int nf, int* eoff, int* bsum, cudaStream_t s);
+void launch_edge_fill(const int* ncount, const int* nlist, int n, int nf, const int* eoff, int* ei, int* ej,
+                      cudaStream_t s);
+// `count` training samples (3 float4 each) of edges drawn at random from the
+// ne CSR edges: features of the pair and its FP64 PressureA + DiffuseInterface
+// + ViscosityV force on i as target (valid = 0 outside every radius or j == i)
+void launch_collect(const SimConst& c, const double4* pos, const double4* press, const double4* gc,
+                    const int* ei, const int* ej, long long ne, long long count, unsigned long long seed,
+                    float4* out, cudaStream_t s);
+// sums over fluid particles of |F_a - F_b|^2, |F_b|^2, |F_b - F_a + L|^2
+void launch_force_compare(int nf, const double4* fa, const double4* fb, const float4* lsum, double* sums3,
+                          cudaStream_t s);
 void launch_virial(const SimConst& c, const double4* pos, const double4* vel, const double4* press,
                    const double4* gc, const int* ncount, const int* nlist, double* virial_p,
                    cudaStream_t s);

@@ -121,7 +121,7 @@ def compute_constants(params: N.Params, header: N.GridHeader, dim: int) -> N.Con
     return c
 
 
-_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED, "mixed_p64": N.MODE_MIXED_P64}
+_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED, "mixed_p64": N.MODE_MIXED_P64, "learned": N.MODE_LEARNED}
 
 
 class Solver:
@@ -157,6 +157,22 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self._lib.mph_synchronize(self._ctx), self._ctx)
+
+    # -- learned form ----------------------------------------------------
+    def set_learned(self, model, judge_interval: int = 20, tolerance: float = 1e-2) -> None:
+        """Attach an edge-MLP model (mphexplicit_b200.learned.Model) to a
+        "learned" solver; the plain FP64 step judges every judge_interval steps."""
+        _check(self._lib.mph_set_learned(self._ctx, model.handle, int(judge_interval), float(tolerance)), self._ctx)
+        self._model = model  # the context keeps a reference
+
+    def learned_stats(self) -> dict:
+        i = N.LearnedInfo()
+        _check(self._lib.mph_learned_stats(self._ctx, C.byref(i)), self._ctx)
+        return {k: getattr(i, k) for k, _ in N.LearnedInfo._fields_}
+
+    def collect_samples(self, dataset, count: int, seed: int = 0) -> None:
+        """Append `count` random edges of the current state to the dataset."""
+        _check(self._lib.mph_collect_samples(self._ctx, dataset.handle, int(count), int(seed)), self._ctx)
 
     # -- read-back -------------------------------------------------------
     def info(self) -> dict:
