@@ -340,7 +340,8 @@ typedef struct mph_learned_info {
     long long plain_steps;     /* steps taken by the plain step after a fallback */
     double last_force_error;   /* relative L2 error of the fluid forces        */
     double max_force_error;
-    double last_term_error;    /* relative L2 error of the replaced terms      */
+    double last_term_error;    /* relative L2 error of the replaced terms (0
+                                  when they are below 1e-6 of the total force) */
     double max_term_error;
 } mph_learned_info;
 int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);

@@ -777,12 +777,18 @@ static int step_learned(mph_ctx* ctx, int nsteps) {
                 std::string merr;
                 if (mph::mlp::model_error_flag(md, &merr) != 0) return fail(ctx, MPH_ERR_DEVICE, merr);
                 const double e = L.h_sums[1] > 0.0 ? std::sqrt(L.h_sums[0] / L.h_sums[1]) : 0.0;
-                const double te = L.h_sums[2] > 0.0 ? std::sqrt(L.h_sums[0] / L.h_sums[2]) : 0.0;
                 ++L.info.judged;
                 L.info.last_force_error = e;
-                L.info.last_term_error = te;
                 L.info.max_force_error = std::max(L.info.max_force_error, e);
-                L.info.max_term_error = std::max(L.info.max_term_error, te);
+                // the replaced terms' own relative error, where they are not
+                // negligible against the total force (a fluid at rest has none)
+                if (L.h_sums[2] > 1e-12 * L.h_sums[1]) {
+                    const double te = std::sqrt(L.h_sums[0] / L.h_sums[2]);
+                    L.info.last_term_error = te;
+                    L.info.max_term_error = std::max(L.info.max_term_error, te);
+                } else {
+                    L.info.last_term_error = 0.0;
+                }
                 if (!(e <= L.tol)) {  // fall back: take the judge's step
                     use = false;
                     ++L.info.fallbacks;
