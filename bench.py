@@ -57,6 +57,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_bf16_peak() -> float:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["bf16_tflops"])
+    return 1590.0
+
+
 def ncu_traffic(kernel: str, mode: str):
     """DRAM bytes per step of the `kernel` scope on the full-size dam break,
     from the committed ncu summary (profiles/), or None."""
@@ -112,6 +120,107 @@ class ClockSampler:
                           and "Not" not in r[5 + k]})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+# edge-MLP flops per evaluated edge: 2 * (9*128 + 128*128 + 128*128 + 128*3)
+MLP_FLOPS_PER_EDGE = 2.0 * (9 * 128 + 128 * 128 * 2 + 128 * 3)
+
+
+def measure_learned(args, rank):
+    """The learned form on the 1 M-fluid dam break (80x80x160 fluid in a
+    240x80x192-cell box): training data from the FP64 step on 8 seeded
+    jitters (2000 FP64 steps in all, spread over the first ~1100 steps of the
+    flow by an untimed pre-roll in the FP64-core mixed form), Adam training of
+    the edge MLP on the tensor cores, then a timed run of `learned_steps`
+    steps with the plain FP64 step as judge every 20 steps (fallback above a
+    relative force error of 1e-2), and its velocity error against the FP64 run
+    of the same steps."""
+    import torch
+    import mphexplicit_b200 as M
+    from mphexplicit_b200 import learned as LR
+    from mphexplicit_b200 import scenes
+
+    def scene(seed):
+        return scenes.dam_break_3d(fluid=(80, 80, 160), box=(240, 80, 192), seed=seed)
+
+    t0 = time.perf_counter()
+    seeds = 8
+    per = max(1, args.learn_steps // seeds)
+    every = max(1, per // 10)
+    samples = 1 << 16
+    ds = LR.Dataset(seeds * (per // every + 1) * samples)
+    for k in range(seeds):
+        sc = scene(1000 + rank * 100 + k)
+        start = (k * 1000) // seeds  # spread the seeds over the first 1000 steps
+        if start > 0:
+            pre = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode="mixed_p64")
+            pre.step(start)
+            st = pre.state()
+            pre.close()
+            order = np.argsort(st["particle_index"], kind="stable")
+            x0, v0, t0_ = st["xyz"][order], st["vel"][order], st["type"][order]
+        else:
+            x0, v0, t0_ = sc.xyz, sc.vel, sc.type
+        s = M.Solver(sc.params, sc.header, t0_, x0, v0, dim=3, mode="fp64")
+        for q in range(0, per, every):
+            s.collect_samples(ds, samples, seed=k * 100003 + q)
+            s.step(min(every, per - q))
+        s.close()
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    m = LR.Model(seed=rank)
+    m.fit_scales(ds)
+    loss = m.train(ds, epochs=args.learn_epochs, batch=4096, lr=2e-3, seed=rank)
+    t_train = time.perf_counter() - t0
+    n_samples = len(ds)
+    ds.close()
+
+    sc = scene(rank)
+    steps = args.learned_steps
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode="learned")
+    s.set_learned(m, 20, 1e-2)
+    s.step(3)  # warm-up (counted in the judge's statistics)
+    s.synchronize()
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.profile(True)
+    ev0.record(stream)
+    s.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    prof = s.profile_read()
+    stats = s.learned_stats()
+    got = s.state()
+    s.close()
+    ref = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode="fp64")
+    ref.step(3 + steps)
+    rst = ref.state()
+    ref.close()
+    o1, o2 = np.argsort(got["particle_index"]), np.argsort(rst["particle_index"])
+    fl = rst["type"][o2] < 2
+    err = float(np.linalg.norm(got["vel"][o1][fl] - rst["vel"][o2][fl]) / np.linalg.norm(rst["vel"][o2][fl]))
+    m.close()
+    out = {"workload": "dam_break_3d fluid 80x80x160 in a 240x80x192-cell box: %d particles (%d fluid)"
+                       % (sc.n, sc.n_fluid),
+           "value": sc.n_fluid * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+           "rel_l2_vel_vs_fp64": err, "error_steps": 3 + steps,
+           "judge_interval": 20, "tolerance": 1e-2,
+           "fallback_rate": stats["plain_steps"] / max(1, stats["steps"]), "judge": stats,
+           "kernels_ms_per_step": {k: v[1] / steps for k, v in prof.items()},
+           "training": {"fp64_steps": seeds * per, "seeds": seeds, "samples": n_samples, "epochs": args.learn_epochs,
+                        "final_loss": loss, "data_s": t_data, "train_s": t_train}}
+    if "mlp_edges" in prof:
+        nl, tot = prof["mlp_edges"]
+        avg_s = tot / max(1, nl) / 1e3
+        tflops = stats["edges"] * MLP_FLOPS_PER_EDGE / avg_s / 1e12
+        peak = measured_bf16_peak()
+        out["roofline"] = {"kernel": "mlp_edges", "bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                           "frac": tflops / peak, "edges_per_launch": stats["edges"],
+                           "flops_per_edge": MLP_FLOPS_PER_EDGE, "avg_launch_ms": avg_s * 1e3,
+                           "peak_source": "measured bf16 burst (MEASURED_PEAKS.json)"}
+    return out
 
 
 def make_scene(args, rank):
@@ -264,6 +373,10 @@ def main():
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--learned", type=int, default=1, help="measure the learned form (config 5) too")
+    ap.add_argument("--learned-steps", type=int, default=1000)
+    ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
+    ap.add_argument("--learn-epochs", type=int, default=4)
     ap.add_argument("--preroll", type=int, default=500,
                     help="untimed steps before the warm-up, so the timed window sees the neighbour "
                          "rebuilds of the developed flow (a dam break at rest rebuilds rarely)")
@@ -305,6 +418,9 @@ def main():
             f["error_steps"] = args.preroll + max(args.warmup, 3) + args.steps
             f["speedup_vs_fp64"] = ref["ms"] / r["ms"]
         forms[m] = f
+
+    if args.learned and not args.only:
+        forms["learned"] = measure_learned(args, rank)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

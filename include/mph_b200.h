@@ -343,6 +343,7 @@ typedef struct mph_learned_info {
     double last_term_error;    /* relative L2 error of the replaced terms (0
                                   when they are below 1e-6 of the total force) */
     double max_term_error;
+    long long edges;           /* CSR edges the network evaluates per step     */
 } mph_learned_info;
 int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);
 

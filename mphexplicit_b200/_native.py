@@ -130,7 +130,8 @@ class LearnedInfo(C.Structure):
 
     _fields_ = [("steps", C.c_longlong), ("learned_steps", C.c_longlong), ("judged", C.c_longlong),
                 ("fallbacks", C.c_longlong), ("plain_steps", C.c_longlong), ("last_force_error", C.c_double),
-                ("max_force_error", C.c_double), ("last_term_error", C.c_double), ("max_term_error", C.c_double)]
+                ("max_force_error", C.c_double), ("last_term_error", C.c_double), ("max_term_error", C.c_double),
+                ("edges", C.c_longlong)]
 
 
 # every symbol the header declares, with its ctypes signature

@@ -76,10 +76,18 @@ constexpr uint32_t ID_GW = tc::idesc_bf16(128, 128, true, true);
 constexpr uint32_t ID_GB = tc::idesc_bf16(128, 16, true, false);
 constexpr uint32_t ID_G1 = tc::idesc_bf16(128, 16, true, true);
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z / 2)) / 2 with the hardware tanh approximation
+// (relative error ~2^-11, below the BF16 rounding of every activation)
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
+    const float s = sigmoid(z);
+    return s * fmaf(z, 1.0f - s, 1.0f);
 }
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -119,10 +127,12 @@ __device__ __forceinline__ void store_x(uint8_t* sx, int e, const float* f) {
     st_row16(sx, e, 0, KIN, p);
 }
 
-// forward epilogue of a hidden layer: Z = D + b -> (bf16) zbuf, H = silu(Z) -> hbuf
-__device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias, uint8_t* zbuf, uint8_t* hbuf, int e) {
+// forward epilogue of a hidden layer: Z = D + b -> (bf16) zbuf, H = silu(Z) -> hbuf,
+// columns [16 c0, 16 c1) of row e
+__device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias, uint8_t* zbuf, uint8_t* hbuf, int e,
+                                           int c0 = 0, int c1 = H / 16) {
 #pragma unroll 1
-    for (int c = 0; c < H / 16; ++c) {
+    for (int c = c0; c < c1; ++c) {
         float v[16];
         tc::tmem_ld16(trow + T_D + 16 * c, v);
         uint32_t zp[8], hp[8];
@@ -365,16 +375,19 @@ k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 // Inference: the network on every row; SRC 0 takes the rows from training
 // samples, SRC 1 builds them from the FP64 state along the CSR edges of the
 // fluid particles.  out[g] = (fx, fy, fz, 0) in N, zero for masked rows.
+// 256 threads: warpgroup 0 builds the rows and writes the outputs; the two
+// warpgroups share each epilogue (columns 0-63 and 64-127 of the same rows:
+// warps w and w+4 read the same TMEM lane quarter).
 template <int SRC>
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(256, 2)
 k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ samples, long long n, EdgeSource es,
             Scales sc, float4* __restrict__ out, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t sm[];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, row = tid & 127;
     {
         const uint4* src = reinterpret_cast<const uint4*>(image);
         uint4* dst = reinterpret_cast<uint4*>(sm + S_W);
-        for (int k = tid; k < PK_BYTES / 16; k += 128) dst[k] = src[k];
+        for (int k = tid; k < PK_BYTES / 16; k += 256) dst[k] = src[k];
     }
     const float* b1 = reinterpret_cast<const float*>(sm + S_W + PK_B);
     const float* b2 = b1 + H;
@@ -389,11 +402,12 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tb = *tslot;
-    const uint32_t trow = tb + ((uint32_t)(warp * 32) << 16);
+    const uint32_t trow = tb + ((uint32_t)((warp & 3) * 32) << 16);
     const uint32_t aW1 = tc::smem_addr(sm + S_W + PK_W1), aW2 = tc::smem_addr(sm + S_W + PK_W2);
     const uint32_t aW3 = tc::smem_addr(sm + S_W + PK_W3), aW4 = tc::smem_addr(sm + S_W + PK_W4);
     const uint32_t aX = tc::smem_addr(sm + I_X), aH = tc::smem_addr(sm + I_H);
     constexpr uint32_t TD4 = 128;
+    const int c0 = wg * (H / 32), c1 = c0 + H / 32;  // this warpgroup's 16-column chunks
 
     uint32_t phase = 0;
     bool ok = true;
@@ -414,10 +428,10 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
     const long long rows = SRC == 0 ? n : es.ne;
     const long long ntiles = (rows + TILE - 1) / TILE;
     for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const long long g = t * TILE + tid;
+        const long long g = t * TILE + row;
         float f[NIN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         bool valid = false;
-        if (g < rows) {
+        if (wg == 0 && g < rows) {
             if (SRC == 0) {
                 float tg[3];
                 valid = sample_features(samples, g, sc, f, tg);
@@ -450,22 +464,22 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 #pragma unroll
             for (int k = 0; k < NIN; ++k) f[k] = 0.f;
         }
-        store_x(sm + I_X, tid, f);
+        if (wg == 0) store_x(sm + I_X, row, f);
         run([&] { tc::mma_bf16(tb + T_D, tc::desc_k(aX, KIN), tc::desc_k(aW1, KIN), ID_F128, 0u); });
         if (!ok) break;
-        epi_hidden(trow, b1, nullptr, sm + I_H, tid);
+        epi_hidden(trow, b1, nullptr, sm + I_H, row, c0, c1);
         run([&] {
             for (int s = 0; s < H / 16; ++s)
                 tc::mma_bf16(tb + T_D, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW2 + 256 * s, H), ID_F128, s > 0);
         });
         if (!ok) break;
-        epi_hidden(trow, b2, nullptr, sm + I_H, tid);
+        epi_hidden(trow, b2, nullptr, sm + I_H, row, c0, c1);
         run([&] {
             for (int s = 0; s < H / 16; ++s)
                 tc::mma_bf16(tb + T_D, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW3 + 256 * s, H), ID_F128, s > 0);
         });
         if (!ok) break;
-        epi_hidden(trow, b3, nullptr, sm + I_H, tid);
+        epi_hidden(trow, b3, nullptr, sm + I_H, row, c0, c1);
         run([&] {
             for (int s = 0; s < H / 16; ++s)
                 tc::mma_bf16(tb + TD4, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW4 + 256 * s, H), ID_F16, s > 0);
@@ -473,7 +487,7 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
         if (!ok) break;
         float v[16];
         tc::tmem_ld16(trow + TD4, v);
-        if (g < rows) {
+        if (wg == 0 && g < rows) {
             out[g] = valid ? make_float4((v[0] + b4[0]) * sc.f_scale, (v[1] + b4[1]) * sc.f_scale,
                                          (v[2] + b4[2]) * sc.f_scale, 0.f)
                            : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -672,7 +686,7 @@ int model_predict(Model* m, const float4* samples, long long n, float4* out, std
     const long long ntiles = (n + TILE - 1) / TILE;
     const int ctas = (int)std::min<long long>(2LL * m->ctas, ntiles);
     EdgeSource es{};
-    k_mlp_infer<0><<<ctas, 128, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err);
+    k_mlp_infer<0><<<ctas, 256, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err);
     MTRY(cudaGetLastError());
     return check_flag(m, err);
 }
@@ -683,7 +697,7 @@ int model_apply_edges(Model* m, const EdgeSource& src, float4* out, cudaStream_t
     if (src.ne <= 0) return 0;
     const long long ntiles = (src.ne + TILE - 1) / TILE;
     const int ctas = (int)std::min<long long>(2LL * m->ctas, ntiles);
-    k_mlp_infer<1><<<ctas, 128, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err);
+    k_mlp_infer<1><<<ctas, 256, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err);
     MTRY(cudaGetLastError());
     if (launches) *launches = 1;
     return 0;

@@ -825,6 +825,7 @@ extern "C" int mph_set_learned(mph_ctx* ctx, mph_model* m, int judge_interval, d
 extern "C" int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info) {
     if (!ctx || !info) return fail(ctx, MPH_ERR_ARG, "bad arguments");
     *info = ctx->lrn.info;
+    info->edges = ctx->lrn.ne;
     return MPH_OK;
 }
 
