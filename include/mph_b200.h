@@ -347,6 +347,60 @@ typedef struct mph_learned_info {
 } mph_learned_info;
 int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);
 
+/* ---- batched form: many independent scenes in one step -----------------
+ * No counterpart in the reference, which runs one scene per process; each
+ * scene here takes the reference's step (main.cpp:386-431, the start-up sort
+ * of main.cpp:357-359 included) with the mixed form's FP32 pair arithmetic
+ * and FP64 integration.  All scenes of a batch have the same dimension; walls
+ * must be static (zero Wall2/3 Velocity and Omega).  Scene s keeps its own
+ * *.data parameters, domain and cell grid; a step advances every scene by its
+ * own dt.  The sweeps are persistent kernels over (scene, cell tile) work
+ * items; mph_batch_step replays steps as captured CUDA graphs of
+ * MPH_BATCH_GRAPH_STEPS steps (the remainder as direct launches). */
+#define MPH_BATCH_GRAPH_STEPS 16
+typedef struct mph_batch mph_batch;
+
+/* headers[s].particle_count particles per scene; type, xyz[3], vel[3] hold
+ * the scenes' particles one scene after the other, each in its *.grid order. */
+int mph_batch_create(int n_scenes, const mph_params* params, const mph_grid_header* headers, int dim,
+                     const int* type, const double* xyz, const double* vel, mph_batch** out);
+/* Enqueue nsteps steps of every scene on the batch's stream (asynchronous). */
+int mph_batch_step(mph_batch* b, int nsteps);
+/* Wait for the stream; MPH_ERR_CAPACITY / MPH_ERR_NONFINITE from the device flags. */
+int mph_batch_synchronize(mph_batch* b);
+/* Positions and velocities of every scene in its input order (layout of
+ * mph_batch_create's xyz / vel). */
+int mph_batch_get_state(mph_batch* b, double* xyz, double* vel);
+/* Cell tile (tz ignored in 2-D) and CTA size of the sweeps. */
+int mph_batch_set_tiles(mph_batch* b, int tx, int ty, int tz, int threads);
+typedef struct mph_batch_trial {
+    int tile[3];
+    int threads;
+    double ms_per_step;
+} mph_batch_trial;
+/* Time every candidate tile shape and CTA size on the batch itself for about
+ * `steps` steps each, keep the fastest, and put the batch state back as it
+ * was: the simulation does not advance.  trials[capacity] receives the
+ * timings (may be NULL), *count the number of candidates timed. */
+int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* trials, int capacity, int* count);
+typedef struct mph_batch_info {
+    int dim, scenes, particles, fluid_particles;
+    int tile[3];
+    int threads, items, capacity, grid_a, grid_b, graph_steps;
+    long long steps;            /* steps taken                                   */
+    long long scene_rebuilds;   /* per-scene cell sorts since creation            */
+    long long tile_splits;      /* tiles split because their halo did not fit     */
+    long long launches;         /* kernels launched                               */
+} mph_batch_info;
+int mph_batch_get_info(mph_batch* b, mph_batch_info* info);
+void* mph_batch_stream(mph_batch* b);
+/* Per-kernel-group CUDA-event timing of subsequent steps (direct launches
+ * instead of graphs while enabled); read as for mph_profile_read. */
+int mph_batch_profile_enable(mph_batch* b, int enable);
+int mph_batch_profile_read(mph_batch* b, mph_kernel_stat* out, int capacity, int* count);
+int mph_batch_last_error(mph_batch* b, char* buf, int len);
+void mph_batch_destroy(mph_batch* b);
+
 /* Last error message of ctx (or of the calling thread if ctx is NULL). */
 int mph_last_error(mph_ctx* ctx, char* buf, int len);
 

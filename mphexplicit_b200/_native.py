@@ -134,6 +134,23 @@ class LearnedInfo(C.Structure):
                 ("edges", C.c_longlong)]
 
 
+class BatchTrial(C.Structure):
+    """mph_batch_trial: one candidate of the batch autotuner."""
+
+    _fields_ = [("tile", C.c_int * 3), ("threads", C.c_int), ("ms_per_step", C.c_double)]
+
+
+class BatchInfo(C.Structure):
+    """mph_batch_info: shape and counters of a batch."""
+
+    _fields_ = [("dim", C.c_int), ("scenes", C.c_int), ("particles", C.c_int), ("fluid_particles", C.c_int),
+                ("tile", C.c_int * 3), ("threads", C.c_int), ("items", C.c_int), ("capacity", C.c_int),
+                ("grid_a", C.c_int), ("grid_b", C.c_int), ("graph_steps", C.c_int), ("steps", C.c_longlong),
+                ("scene_rebuilds", C.c_longlong), ("tile_splits", C.c_longlong), ("launches", C.c_longlong)]
+
+
+BATCH_GRAPH_STEPS = 16
+
 # every symbol the header declares, with its ctypes signature
 _P = C.c_void_p
 _I = C.c_int
@@ -188,6 +205,18 @@ SIGNATURES = {
     "mph_collect_samples": (_I, [_P, _P, C.c_longlong, C.c_ulonglong]),
     "mph_set_learned": (_I, [_P, _P, _I, C.c_double]),
     "mph_learned_stats": (_I, [_P, C.POINTER(LearnedInfo)]),
+    "mph_batch_create": (_I, [_I, C.POINTER(Params), C.POINTER(GridHeader), _I, _ip, _dp, _dp, C.POINTER(_P)]),
+    "mph_batch_step": (_I, [_P, _I]),
+    "mph_batch_synchronize": (_I, [_P]),
+    "mph_batch_get_state": (_I, [_P, _dp, _dp]),
+    "mph_batch_set_tiles": (_I, [_P, _I, _I, _I, _I]),
+    "mph_batch_autotune": (_I, [_P, _I, C.POINTER(BatchTrial), _I, _ip]),
+    "mph_batch_get_info": (_I, [_P, C.POINTER(BatchInfo)]),
+    "mph_batch_stream": (_P, [_P]),
+    "mph_batch_profile_enable": (_I, [_P, _I]),
+    "mph_batch_profile_read": (_I, [_P, C.POINTER(KernelStat), _I, _ip]),
+    "mph_batch_last_error": (_I, [_P, C.c_char_p, _I]),
+    "mph_batch_destroy": (None, [_P]),
     "mph_last_error": (_I, [_P, C.c_char_p, _I]),
     "mph_destroy": (None, [_P]),
     "mph_version": (C.c_char_p, []),

@@ -246,37 +246,34 @@ extern "C" int mph_compute_constants(const mph_params* p, const mph_grid_header*
 }
 
 // Kernel constants derived from mph_constants, in the reference's order.
-static int fill_simconst(mph_ctx* ctx) {
-    const mph_constants& c = ctx->c;
-    const mph_params& p = ctx->p;
-    SimConst& s = ctx->sc;
+int mph::make_simconst(const mph_params& p, const mph_grid_header& h, const mph_constants& c, int dim, int n,
+                       SimConst& s, std::string& msg) {
     std::memset(&s, 0, sizeof(s));
-    const int dim = ctx->dim;
-    const double l0 = ctx->h.particle_spacing;
-    s.n = ctx->n;
+    const double l0 = h.particle_spacing;
+    s.n = n;
     s.dim = dim;
     s.tot = c.total_cell_count;
     for (int d = 0; d < 3; ++d) {
         s.cc[d] = c.cell_count[d];
-        s.dmin[d] = ctx->h.domain_min[d];
+        s.dmin[d] = h.domain_min[d];
         s.width[d] = c.domain_width[d];
         s.half_width[d] = 0.5 * c.domain_width[d];
         s.cell_width[d] = c.cell_width[d];
     }
     if (s.cc[0] < 1 || s.cc[1] < 1 || s.cc[2] < 1 || s.tot < 1)
-        return fail(ctx, MPH_ERR_GEOMETRY, "domain narrower than one cell of MaxRadius+MARGIN");
+        { msg = "domain narrower than one cell of MaxRadius+MARGIN"; return MPH_ERR_GEOMETRY; }
     if ((long long)s.cc[0] * s.cc[1] * s.cc[2] > (1LL << 29))
-        return fail(ctx, MPH_ERR_GEOMETRY, "too many cells");
+        { msg = "too many cells"; return MPH_ERR_GEOMETRY; }
     const double rm = c.max_radius + 0.1 * l0;  // MaxRadius + MARGIN
     s.rm2 = rm * rm;
     s.range[0] = (int)std::ceil(rm / c.cell_width[0]);
     s.range[1] = (int)std::ceil(rm / c.cell_width[1]);
     s.range[2] = dim == 2 ? 0 : (int)std::ceil(rm / c.cell_width[2]);
     for (int d = 0; d < 3; ++d)  // the reference asserts 2*range+1 <= 3 (main.cpp:1347-1349)
-        if (2 * s.range[d] + 1 > 3) return fail(ctx, MPH_ERR_GEOMETRY, "cell narrower than MaxRadius+MARGIN");
+        if (2 * s.range[d] + 1 > 3) { msg = "cell narrower than MaxRadius+MARGIN"; return MPH_ERR_GEOMETRY; }
     int pe = 0;
-    while ((ctx->n >> pe) != 0) ++pe;  // smallest power of two above n (main.cpp:612-617)
-    if (pe > 30) return fail(ctx, MPH_ERR_ARG, "too many particles");
+    while ((n >> pe) != 0) ++pe;  // smallest power of two above n (main.cpp:612-617)
+    if (pe > 30) { msg = "too many particles"; return MPH_ERR_ARG; }
     s.pow2 = 1 << pe;
     s.dt = p.dt;
     s.l0 = l0;
@@ -329,6 +326,13 @@ static int fill_simconst(mph_ctx* ctx) {
         }
     }
     for (int d = 0; d < 3; ++d) s.gravity[d] = p.gravity[d];
+    return MPH_OK;
+}
+
+static int fill_simconst(mph_ctx* ctx) {
+    std::string msg;
+    const int st = mph::make_simconst(ctx->p, ctx->h, ctx->c, ctx->dim, ctx->n, ctx->sc, msg);
+    if (st != MPH_OK) return fail(ctx, st, msg);
     return MPH_OK;
 }
 

@@ -145,6 +145,12 @@ int check_division(unsigned long long seed, long long n, unsigned long long* d_c
 void launch_conserved(const SimConst& c, const int* cellstart, const double4* pos,
                       const double4* vel, double* out5, cudaStream_t s);
 
+// Kernel constants of one scene from its parameters, header and set-up
+// constants (mph_compute_constants), evaluated in the reference's order
+// (mph_host.cpp); on failure returns the status and sets msg.
+int make_simconst(const mph_params& p, const mph_grid_header& h, const mph_constants& c, int dim, int n,
+                  SimConst& s, std::string& msg);
+
 // Sets the calling thread's message for mph_last_error(NULL, ...) and returns code.
 int set_thread_error(int code, const std::string& msg);
 

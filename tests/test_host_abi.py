@@ -188,3 +188,31 @@ def test_benchmark_scene_sizes():
     assert np.array_equal(scenes.droplet_2d(seed=5).xyz, scenes.droplet_2d(seed=5).xyz)
     b = scenes.droplet_batch_2d(count=8, seed=1)
     assert len(b) == 8 and all(20 * 20 <= s.n <= 140 * 140 for s in b)
+
+
+def test_batch_rejects_bad_scenes_before_touching_the_gpu():
+    """mph_batch_create validates every scene on the host first."""
+    good = scenes.droplet_batch_2d(count=2, seed=1, lo=10, hi=12)
+    with pytest.raises(ValueError):
+        M.Batch([])
+    moving = scenes.droplet_batch_2d(count=1, seed=2, lo=10, hi=12)[0]
+    moving.params.wall_velocity[2][0] = 0.1
+    with pytest.raises(M.MphError) as e:
+        M.Batch([good[0], moving])
+    assert e.value.code == N.MPH_ERR_ARG and "static walls" in str(e.value)
+    tiny = scenes.droplet_2d(n=4, box=6.0)  # fewer than 3 cells per axis
+    with pytest.raises(M.MphError) as e:
+        M.Batch([good[1], tiny])
+    assert e.value.code == N.MPH_ERR_GEOMETRY and "scene 1" in str(e.value)
+    bad = scenes.droplet_batch_2d(count=1, seed=3, lo=10, hi=12)[0]
+    bad.type[0] = 7
+    with pytest.raises(M.MphError) as e:
+        M.Batch([bad])
+    assert e.value.code == N.MPH_ERR_ARG
+    nan = scenes.droplet_batch_2d(count=1, seed=4, lo=10, hi=12)[0]
+    nan.xyz[3, 1] = np.nan
+    with pytest.raises(M.MphError):
+        M.Batch([nan])
+    mixed_dim = scenes.dam_break_3d(fluid=(4, 4, 4), box=(8, 6, 8))
+    with pytest.raises(ValueError):
+        M.Batch([good[0], mixed_dim])
