@@ -13,6 +13,7 @@ value = fluid particles x steps / seconds, summed over ranks (replicas: the
 step does not shard, each rank runs its own scene on its own GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed|mixed_p64] [--only]
+                  [--learned 0|1] [--batch 0|1]
   python bench.py --impl reference ...   # the reference's own CPU step, all host threads
 
 One JSON line on rank 0.
@@ -223,6 +224,102 @@ def measure_learned(args, rank):
     return out
 
 
+# algorithmic HBM bytes per particle of the batched 2-D sweeps with surface
+# tension (FP64 state, 2-D): sweep A reads x, v, type (36 B) and writes
+# PressureP, PressureA, GravityCenter (32 B); sweep B reads x, v, type and those
+# (68 B) and writes v (16 B) and, through the next move, x (16 B)  -> 168 B.
+BATCH_ALGO_BYTES = {"batch_sweep_a": 68.0, "batch_sweep_b": 100.0}
+
+
+def measure_batch(args, rank):
+    """The batched form on 256 uneven 2-D droplets (each w x h particles,
+    w, h ~ U[20, 140], l0 = 1e-3 m, mu log-uniform in [1e-3, 1] Pa s, sigma
+    uniform in [0.02, 0.08] N/m, dt = 5e-6 s): autotune, then `batch_steps`
+    steps timed as CUDA-graph replays, a per-kernel pass, the velocity error
+    of a sample of scenes against the FP64 form run alone, and the
+    reference's own step on a sample of the scenes (one after the other)."""
+    import torch
+    import mphexplicit_b200 as M
+    from mphexplicit_b200 import scenes
+    scs = scenes.droplet_batch_2d(count=256, seed=rank)
+    b = M.Batch(scs)
+    trials = b.autotune(steps=32)
+    info0 = b.info()
+    steps = args.batch_steps
+    b.step(max(args.warmup, 3) + 13)  # warm-up: at least one full graph replay
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.stream_handle)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    info1 = b.info()
+    ev0.record(stream)
+    b.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    info2 = b.info()
+    b.profile(True)
+    b.step(32)
+    prof = b.profile_read()
+    b.profile(False)
+    done = info2["steps"] + 32
+    xyz, vel = b.state()
+    off = b.offsets
+    b.close()
+    # error of a sample of scenes against the FP64 form (bit-identical to the reference)
+    errs = []
+    for k in range(0, len(scs), max(1, len(scs) // args.batch_check)):
+        sc = scs[k]
+        s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2, mode="fp64")
+        s.step(done)
+        st = s.state()
+        s.close()
+        order = np.argsort(st["particle_index"], kind="stable")
+        rv = st["vel"][order]
+        gv = vel[off[k]:off[k + 1]]
+        errs.append(float(np.linalg.norm(gv - rv) / np.linalg.norm(rv)))
+    nf = int(sum(sc.n_fluid for sc in scs))
+    name, (nl, tot_ms) = max(prof.items(), key=lambda kv: kv[1][1])
+    avg_s = tot_ms / nl / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = BATCH_ALGO_BYTES.get(name, 0.0) * nf / avg_s / 1e9
+    out = {"workload": "256 uneven 2-D droplets (w, h ~ U[20,140] particles, l0=1e-3, mu log-U[1e-3,1], "
+                       "sigma U[0.02,0.08], dt=5e-6): %d particles" % nf,
+           "value": nf * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
+           "graph_steps": info0["graph_steps"], "tile": list(info0["tile"]), "threads": info0["threads"],
+           "items": info0["items"], "scene_rebuilds_in_timed_region": info2["scene_rebuilds"] - info1["scene_rebuilds"],
+           "tile_splits": info2["tile_splits"], "autotune": trials,
+           "rel_l2_vel_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "scenes": len(errs),
+                                  "steps": done},
+           "kernels_ms_per_step": {k: v[1] / 32 for k, v in prof.items()},
+           "roofline": {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_source": peak_kind,
+                        "algorithmic_bytes_per_launch": BATCH_ALGO_BYTES.get(name, 0.0) * nf,
+                        "avg_launch_ms": avg_s * 1e3}}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+        threads = os.cpu_count() or 1
+        tot_s, tot_upd, n_sc = 0.0, 0, 0
+        with tempfile.TemporaryDirectory() as td:
+            for k in range(0, len(scs), max(1, len(scs) // args.batch_cpu_scenes)):
+                sc = scs[k]
+                d, g = os.path.join(td, "s.data"), os.path.join(td, "s.grid")
+                sc.write(d, g)
+                if po.ref_available(2):
+                    r = po.time_reference(d, g, 2, 0, args.batch_cpu_steps, threads, timeout=600)
+                    kind = "reference"
+                else:
+                    os.environ["OMP_NUM_THREADS"] = str(threads)
+                    r = po.time_oracle(sc, 0, args.batch_cpu_steps)
+                    kind = "port"
+                tot_s += r["seconds"]
+                tot_upd += r["fluid"] * r["steps"]
+                n_sc += 1
+        out["cpu_baseline"] = {"value": tot_upd / tot_s, "unit": UNIT, "cores": threads, "kind": kind,
+                               "sample": "%d of the 256 scenes, %d steps each, one after the other, %.1f s wall"
+                                         % (n_sc, args.batch_cpu_steps, tot_s)}
+    return out
+
+
 def make_scene(args, rank):
     from mphexplicit_b200 import scenes
     if args.scene == "dam":
@@ -377,6 +474,11 @@ def main():
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
     ap.add_argument("--learn-epochs", type=int, default=4)
+    ap.add_argument("--batch", type=int, default=1, help="measure the batched form (256 2-D droplets) too")
+    ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
+    ap.add_argument("--batch-cpu-scenes", type=int, default=16)
+    ap.add_argument("--batch-cpu-steps", type=int, default=200)
     ap.add_argument("--preroll", type=int, default=500,
                     help="untimed steps before the warm-up, so the timed window sees the neighbour "
                          "rebuilds of the developed flow (a dam break at rest rebuilds rarely)")
@@ -421,6 +523,8 @@ def main():
 
     if args.learned and not args.only:
         forms["learned"] = measure_learned(args, rank)
+    if args.batch and not args.only:
+        forms["batch"] = measure_batch(args, rank)
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -464,18 +464,37 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                 };
                 const bool st = ST && sc.has_st;
                 const bool ratio1 = sc.ratio_all_one;
-                if (SWEEP == 0) {
-                    float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
-                    float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+                // Pairs within sqrt(cut2) in the runs' order: each chunk of up to 64
+                // candidates is filtered into a bit mask first, then only the set
+                // bits are visited, so the lanes of a warp run the pair terms
+                // together instead of under divergent distance tests.
+                auto for_near = [&](float cut2, auto&& visit) {
                     for (int r = 0; r < (DIM == 2 ? 3 : 9); ++r) {
                         int rb, re;
                         run_of(r, rb, re);
-                        for (int j = rb; j < re; ++j) {
-                            if (j == si) continue;
-                            float dx, dy, dz;
-                            disp(j, dx, dy, dz);
-                            const float r2 = dx * dx + dy * dy + dz * dz;
-                            if (r2 > sc.cut2_a) continue;
+                        for (int base = rb; base < re; base += 64) {
+                            const int cnt = min(64, re - base);
+                            unsigned long long m = 0ull;
+                            for (int q = 0; q < cnt; ++q) {
+                                float dx, dy, dz;
+                                disp(base + q, dx, dy, dz);
+                                if (dx * dx + dy * dy + dz * dz < cut2) m |= 1ull << q;
+                            }
+                            if (si >= base && si < base + cnt) m &= ~(1ull << (si - base));
+                            while (m != 0ull) {
+                                const int j = base + __ffsll((long long)m) - 1;
+                                m &= m - 1ull;
+                                float dx, dy, dz;
+                                disp(j, dx, dy, dz);
+                                visit(j, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+                            }
+                        }
+                    }
+                };
+                if (SWEEP == 0) {
+                    float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
+                    float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+                    for_near(sc.cut2_a, [&](int j, float dx, float dy, float dz, float r2) {
                             const float rinv = rsqrt_nr(r2);
                             const float rr = r2 * rinv;
                             if (r2 <= sc.rp2) {
@@ -492,8 +511,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                                 if (ratio1) st_density<false>(sc, ti, tj, r2, rr, dx, dy, dz, sa, cak, g0, g1, g2);
                                 else st_density<true>(sc, ti, tj, r2, rr, dx, dy, dz, sa, cak, g0, g1, g2);
                             }
-                        }
-                    }
+                    });
                     const double strain = (double)((sp - cpk) - sc.n0p);
                     const double div = (double)(sd - cdk);
                     double kappa = sc.bulk_modulus_d[ti];
@@ -518,15 +536,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                     const float mu_u = sc.visc_mu[ti][ti];
                     float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz2 = 0.f;  // short range, Kahan
                     float gx = 0.f, gy = 0.f, gz = 0.f;                                  // long range
-                    for (int r = 0; r < (DIM == 2 ? 3 : 9); ++r) {
-                        int rb, re;
-                        run_of(r, rb, re);
-                        for (int j = rb; j < re; ++j) {
-                            if (j == si) continue;
-                            float dx, dy, dz;
-                            disp(j, dx, dy, dz);
-                            const float r2 = dx * dx + dy * dy + dz * dz;
-                            if (r2 >= sc.cut2_b) continue;
+                    for_near(sc.cut2_b, [&](int j, float dx, float dy, float dz, float r2) {
                             const float rinv = rsqrt_nr(r2);
                             const float rr = r2 * rinv;
                             const float4 vj = sV[j];
@@ -554,8 +564,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                                 gy += fmaf(s, dy, t.y);
                                 if (DIM == 3) gz += fmaf(s, dz, t.z);
                             }
-                        }
-                    }
+                    });
                     double F0 = ((double)fx - (double)cx) + (double)gx;
                     double F1 = ((double)fy - (double)cy) + (double)gy;
                     double F2 = ((double)fz - (double)cz2) + (double)gz;
@@ -733,7 +742,9 @@ static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& 
     s.rp2 = (float)c.rp2;
     s.rv2 = (float)c.rv2;
     s.rg2 = (float)c.rg2;
-    s.cut2_a = c.has_st ? std::max(s.rp2, std::max(s.ra2, s.rg2)) : s.rp2;
+    // the density sums take r^2 <= R^2 (main.cpp:1684), the forces r^2 < R^2:
+    // pairs are selected by r^2 < cut2, so cut2_a is the next float above
+    s.cut2_a = std::nextafter(c.has_st ? std::max(s.rp2, std::max(s.ra2, s.rg2)) : s.rp2, INFINITY);
     s.cut2_b = std::max(s.rp2, s.rv2);
     if (c.has_st) s.cut2_b = std::max(s.cut2_b, std::max(s.ra2, s.rg2));
     s.inv_ra = (float)(1.0 / c.ra);
@@ -821,7 +832,7 @@ static int configure(mph_batch* b, const int t[3], int threads) {
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t budget = std::min<size_t>((size_t)smem_optin, 110 * 1024) - sizeof(BScene) - 2048;
-    int cap = (int)std::min<long long>(max_halo + max_halo / 2 + 64, 1 << 20);
+    int cap = (int)std::min<long long>(max_halo + max_halo / 8 + 32, 1 << 20);
     while (cap > 64 && std::max(mph::sweep_smem(dim, 0, b->has_st, cap, hmax, ncol),
                                 mph::sweep_smem(dim, 1, b->has_st, cap, hmax, ncol)) > budget)
         cap -= 32;
