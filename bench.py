@@ -13,7 +13,7 @@ value = fluid particles x steps / seconds, summed over ranks (replicas: the
 step does not shard, each rank runs its own scene on its own GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed|mixed_p64] [--only]
-                  [--learned 0|1] [--batch 0|1]
+                  [--forms fp64,mixed,mixed_p64,learned,batch]
   python bench.py --impl reference ...   # the reference's own CPU step, all host threads
 
 One JSON line on rank 0.
@@ -141,8 +141,11 @@ def measure_learned(args, rank):
     from mphexplicit_b200 import learned as LR
     from mphexplicit_b200 import scenes
 
+    fluid = tuple(int(v) for v in args.learned_fluid.split(","))
+    box = (3 * fluid[0], fluid[1], (6 * fluid[2]) // 5)
+
     def scene(seed):
-        return scenes.dam_break_3d(fluid=(80, 80, 160), box=(240, 80, 192), seed=seed)
+        return scenes.dam_break_3d(fluid=fluid, box=box, seed=seed)
 
     t0 = time.perf_counter()
     seeds = 8
@@ -203,8 +206,8 @@ def measure_learned(args, rank):
     fl = rst["type"][o2] < 2
     err = float(np.linalg.norm(got["vel"][o1][fl] - rst["vel"][o2][fl]) / np.linalg.norm(rst["vel"][o2][fl]))
     m.close()
-    out = {"workload": "dam_break_3d fluid 80x80x160 in a 240x80x192-cell box: %d particles (%d fluid)"
-                       % (sc.n, sc.n_fluid),
+    out = {"workload": "dam_break_3d fluid %dx%dx%d in a %dx%dx%d-cell box: %d particles (%d fluid)"
+                       % (*fluid, *box, sc.n, sc.n_fluid),
            "value": sc.n_fluid * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps,
            "rel_l2_vel_vs_fp64": err, "error_steps": 3 + steps,
            "judge_interval": 20, "tolerance": 1e-2,
@@ -470,11 +473,12 @@ def main():
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--learned", type=int, default=1, help="measure the learned form (config 5) too")
+    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch",
+                    help="forms to measure (comma list); the headline --mode must be among them for a full line")
+    ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
     ap.add_argument("--learn-epochs", type=int, default=4)
-    ap.add_argument("--batch", type=int, default=1, help="measure the batched form (256 2-D droplets) too")
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
     ap.add_argument("--batch-cpu-scenes", type=int, default=16)
@@ -505,9 +509,9 @@ def main():
     if cvd and "," not in cvd and cvd.isdigit():
         gpu_index = int(cvd)
     sc = make_scene(args, rank)
-    modes = [args.mode] if args.only else ["fp64", "mixed", "mixed_p64"]
+    wanted = [args.mode] if args.only else [f.strip() for f in args.forms.split(",") if f.strip()]
+    modes = [m for m in ("fp64", "mixed", "mixed_p64") if m in wanted]
     res = {m: measure_form(args, sc, m, world, gpu_index, with_e2e=(m == args.mode)) for m in modes}
-    head = res[args.mode]
     forms = {}
     for m, r in res.items():
         f = {"value": r["value"], "ms_per_step": r["ms"] / args.steps, "dominant_kernel": r["roofline"]["kernel"],
@@ -521,10 +525,17 @@ def main():
             f["speedup_vs_fp64"] = ref["ms"] / r["ms"]
         forms[m] = f
 
-    if args.learned and not args.only:
+    if "learned" in wanted:
         forms["learned"] = measure_learned(args, rank)
-    if args.batch and not args.only:
+    if "batch" in wanted:
         forms["batch"] = measure_batch(args, rank)
+    if args.mode not in res:  # a run of the extra forms alone (profiling)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "unit": UNIT, "n_gpus": world, "forms": forms}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    head = res[args.mode]
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

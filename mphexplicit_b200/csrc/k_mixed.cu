@@ -77,6 +77,14 @@ __device__ __forceinline__ double omod_fast(double x, double w) {
 
 __device__ __forceinline__ int pack_cell(int x, int y, int z) { return x | (y << 10) | (z << 20); }
 
+// A particle's 32-byte record {hi position + type, velocity + PressureP} in
+// one 256-bit read-only load: one L1 sector per neighbour instead of two.
+__device__ __forceinline__ void ldg_pv(const float4* __restrict__ pv, int j, float4& p, float4& v) {
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(p.x), "=f"(p.y), "=f"(p.z), "=f"(p.w), "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(pv + 2 * (size_t)j));
+}
+
 // Cell-relative position in two FP32 words.  hi lies on a power-of-two grid g
 // with |hi| < 2^24 g, so hi_j - hi_i + Dhi (also on the grid) is computed
 // exactly; lo = x - hi (|lo| <= g/2) carries the rest.  The pair
@@ -352,7 +360,7 @@ template <bool ST, bool RATIO, bool S64>
 __global__ void __launch_bounds__(128)
 k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p32lo, const float4* __restrict__ v32,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
-        float4* __restrict__ v32p, float4* __restrict__ gca, double* __restrict__ strain_out,
+        float4* __restrict__ pv, float4* __restrict__ gca, double* __restrict__ strain_out,
         double* __restrict__ div_out, double* __restrict__ dens_a_out, double* __restrict__ wall_center,
         const SimConst c, const double4* __restrict__ pos64, const double4* __restrict__ vel64,
         double4* __restrict__ press64) {
@@ -450,7 +458,8 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
         dens_a_out[i] = dens;
         gca[i] = make_float4(g0, g1, g2, pa);
     }
-    v32p[i] = make_float4(vi.x, vi.y, vi.z, (float)pp);
+    pv[2 * (size_t)i] = pi;
+    pv[2 * (size_t)i + 1] = make_float4(vi.x, vi.y, vi.z, (float)pp);
     if (S64) press64[i] = make_double4(vid.x, vid.y, vid.z, pp);
     strain_out[i] = strain;
     div_out[i] = div;
@@ -470,7 +479,7 @@ __global__ void __launch_bounds__(128, PART == 0   ? MPH_MIXB_MINB_SHORT
                                        : PART == 1 ? MPH_MIXB_MINB_LONG
                                                    : MPH_MIXB_MINB_FUSED)
 k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ p32,
-        const float4* __restrict__ p32lo, const float4* __restrict__ v32p, const float4* __restrict__ gca,
+        const float4* __restrict__ p32lo, const float4* __restrict__ pv, const float4* __restrict__ gca,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
         const double4* __restrict__ vel, double4* __restrict__ vel_out, double4* __restrict__ force,
         StepScalars* __restrict__ scal, const double4* __restrict__ pos64, const double4* __restrict__ press64) {
@@ -485,7 +494,7 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     }
     const float4 pi = p32[i];
     const float4 li = p32lo[i];
-    const float4 vi = v32p[i];
+    const float4 vi = pv[2 * (size_t)i + 1];
     const int ti = __float_as_int(pi.w);
     float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
     if (ST) gi = gca[i];
@@ -540,7 +549,8 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     if (PART != 1) for (; k < ns; ++k, lp += n) {
         const unsigned e = __ldg(lp);
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
-        const float4 pj = p32[j];
+        float4 pj, vj;
+        ldg_pv(pv, j, pj, vj);
         const float4 lj = p32lo[j];
         const float4 dh = tb.dhi[code], dl = tb.dlo[code];
         const float dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
@@ -551,7 +561,6 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         const float rinv = rsqrt_nr(r2);
         const float r = r2 * rinv;
         const int tj = __float_as_int(pj.w);
-        const float4 vj = v32p[j];
         float s = 0.0f;
         if (r2 < m.rp2) s += (vi.w + vj.w) * fmaf(m.p_b, r, m.p_a) * rinv;
         if (r2 < m.rv2) {
@@ -607,17 +616,16 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         for (int u = 0; u < U; ++u) e[u] = __ldg(lp + (size_t)u * n);
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int j = (int)(e[u] >> kCodeBits);
-            pj[u] = p32[j];
-            vj[u] = v32p[j];
+            ldg_pv(pv, (int)(e[u] >> kCodeBits), pj[u], vj[u]);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) long_pair(e[u], pj[u], vj[u]);
     }
     for (; k < na; ++k, lp += n) {
         const unsigned e = __ldg(lp);
-        const int j = (int)(e >> kCodeBits);
-        long_pair(e, p32[j], v32p[j]);
+        float4 pj, vj;
+        ldg_pv(pv, (int)(e >> kCodeBits), pj, vj);
+        long_pair(e, pj, vj);
     }
     double4 fs;
     if (PART == 1) {
@@ -700,7 +708,7 @@ struct MixedState {
     float4* p32 = nullptr;
     float4* p32lo = nullptr;
     float4* v32 = nullptr;
-    float4* v32p = nullptr;
+    float4* pv = nullptr;  // [2n]: {p32, (v, PressureP)} per particle, written by sweep A
     float4* gca = nullptr;
     unsigned* list = nullptr;
     int cap = 0;
@@ -713,7 +721,7 @@ struct MixedState {
 };
 
 static void mfree(MixedState* m) {
-    void* ptrs[] = {m->keys_unsorted, m->slot, m->counts, m->tmp, m->home, m->p32, m->p32lo, m->v32, m->v32p,
+    void* ptrs[] = {m->keys_unsorted, m->slot, m->counts, m->tmp, m->home, m->p32, m->p32lo, m->v32, m->pv,
                     m->gca, m->list, m->cnt_short, m->cnt_all};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -789,7 +797,7 @@ void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wa
     double* wc = advance_wall ? d.wall_center : nullptr;
 #define MIX_A(ST, RATIO, S64)                                                                                   \
     k_mix_a<ST, RATIO, S64><<<nb, 128, 0, s>>>(m->mc, m->p32, m->p32lo, m->v32, m->list, m->cnt_short,          \
-                                               m->cnt_all, m->v32p, m->gca, d.strain_p, d.div_p, d.dens_a, wc, c, \
+                                               m->cnt_all, m->pv, m->gca, d.strain_p, d.div_p, d.dens_a, wc, c, \
                                                d.pos[d.cur], d.vel[d.vcur], d.press)
 #define MIX_A2(ST, RATIO) \
     if (m->s64) MIX_A(ST, RATIO, true); else MIX_A(ST, RATIO, false)
@@ -809,7 +817,7 @@ static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t 
     double4* vout = WALLS ? nullptr : d.vel[1 - d.vcur];
 #define MIX_B1(ST, RATIO, S64, PART)                                                                        \
     k_mix_b<ST, RATIO, WALLS, S64, PART><<<nb, 128, 0, s>>>(                                              \
-        m->mc, c, d.cellstart, m->p32, m->p32lo, m->v32p, m->gca, m->list, m->cnt_short, m->cnt_all,     \
+        m->mc, c, d.cellstart, m->p32, m->p32lo, m->pv, m->gca, m->list, m->cnt_short, m->cnt_all,     \
         d.vel[d.vcur], vout, d.force, d.scal, d.pos[d.cur], d.press)
 #define MIX_B2(ST, RATIO)             \
     if (m->s64) {                     \
@@ -939,7 +947,7 @@ int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, De
     if (e == cudaSuccess) e = malloc_n(&m->p32, n);
     if (e == cudaSuccess) e = malloc_n(&m->p32lo, n);
     if (e == cudaSuccess) e = malloc_n(&m->v32, n);
-    if (e == cudaSuccess) e = malloc_n(&m->v32p, n);
+    if (e == cudaSuccess) e = malloc_n(&m->pv, 2 * n);
     if (e == cudaSuccess) e = malloc_n(&m->gca, n);
     if (e == cudaSuccess) e = malloc_n(&m->cnt_short, n);
     if (e == cudaSuccess) e = malloc_n(&m->cnt_all, n);
