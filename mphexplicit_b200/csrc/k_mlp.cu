@@ -50,12 +50,16 @@ constexpr int S_TRAIN = S_MISC + 256;
 static_assert(PK_BYTES <= S_X, "image overlaps the input tile");
 static_assert(S_TRAIN <= 227 * 1024, "training kernel exceeds the shared memory of a CTA");
 
-// shared memory of the inference kernel
-constexpr int I_X = S_X;
-constexpr int I_H = I_X + TILE * KIN * 2;
-constexpr int I_MISC = I_H + TILE * H * 2;
+// shared memory of the inference kernel: the weight image once, then for
+// each warpgroup (one 128-edge tile in flight each) its input tile X and its
+// hidden activations H
+constexpr int I_WG = 4;                                      // tiles in flight per CTA
+constexpr int I_TILE_BYTES = TILE * KIN * 2 + TILE * H * 2;  // X + H of one tile
+constexpr int I_T = S_X;
+constexpr int I_MISC = I_T + I_WG * I_TILE_BYTES;
 constexpr int S_INFER = I_MISC + 64;
-static_assert(2 * (S_INFER + 1024) <= 228 * 1024, "two inference CTAs must fit on an SM");
+static_assert(S_INFER <= 227 * 1024, "the inference CTA exceeds the shared memory of a CTA");
+static_assert(I_T % 128 == 0 && I_TILE_BYTES % 128 == 0, "operand tiles must stay 128-byte aligned");
 
 // TMEM columns
 constexpr uint32_t T_D = 0;      // layer output / backward dH  [128 x 128]
@@ -84,7 +88,6 @@ __device__ __forceinline__ float tanh_approx(float x) {
     return y;
 }
 __device__ __forceinline__ float sigmoid(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
-__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigmoid(z);
     return s * fmaf(z, 1.0f - s, 1.0f);
@@ -94,6 +97,21 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 __device__ __forceinline__ float lo_bf(uint32_t p) { return __uint_as_float(p << 16); }
+
+// SiLU of two BF16 activations at once, h = z * (1 + tanh(z/2)) / 2 in packed
+// BF16 arithmetic: z/2 (exact), the hardware's packed tanh approximation,
+// s = bf16(t/2 + 1/2), h = bf16(z * s).  One special-function operation per
+// two activations (the FP32 form takes one each, and that pipe bounds the
+// epilogues); the forward passes of training and inference both use it.
+__device__ __forceinline__ uint32_t silu2(uint32_t z2) {
+    const uint32_t half2 = 0x3F003F00u;  // (0.5, 0.5) in BF16
+    uint32_t hz, t, sg, h;
+    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(hz) : "r"(z2), "r"(half2));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hz));
+    asm("fma.rn.bf16x2 %0, %1, %2, %2;" : "=r"(sg) : "r"(t), "r"(half2));
+    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(h) : "r"(z2), "r"(sg));
+    return h;
+}
 __device__ __forceinline__ float hi_bf(uint32_t p) { return __uint_as_float(p & 0xFFFF0000u); }
 
 // 16 consecutive bf16 of row r, columns c0..c0+15 of a core-layout tile with C columns
@@ -139,7 +157,7 @@ __device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias, uin
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             zp[j] = pack2(v[2 * j] + bias[16 * c + 2 * j], v[2 * j + 1] + bias[16 * c + 2 * j + 1]);
-            hp[j] = pack2(silu(lo_bf(zp[j])), silu(hi_bf(zp[j])));
+            hp[j] = silu2(zp[j]);
         }
         if (zbuf) st_row16(zbuf, e, 16 * c, H, zp);
         st_row16(hbuf, e, 16 * c, H, hp);
@@ -162,7 +180,7 @@ __device__ __forceinline__ void epi_back(uint32_t trow, uint8_t* zbuf, const uin
             uint32_t qp[8], hp[8];
             ld_row16(zprev, e, 16 * c, H, qp);
 #pragma unroll
-            for (int j = 0; j < 8; ++j) hp[j] = pack2(silu(lo_bf(qp[j])), silu(hi_bf(qp[j])));
+            for (int j = 0; j < 8; ++j) hp[j] = silu2(qp[j]);
             st_row16(hbuf, e, 16 * c, H, hp);
         }
     }
@@ -378,8 +396,29 @@ k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 // 256 threads: warpgroup 0 builds the rows and writes the outputs; the two
 // warpgroups share each epilogue (columns 0-63 and 64-127 of the same rows:
 // warps w and w+4 read the same TMEM lane quarter).
+// Named barrier of one warpgroup (ids 1..4; 0 is __syncthreads), plain and
+// with an AND reduction of a predicate.
+__device__ __forceinline__ void wg_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool wg_sync_and(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+// Inference: Y = MLP(X) for rows of `samples` (SRC 0) or for the CSR edges of
+// `es` (SRC 1, features computed from the FP64 state).  One CTA per SM, four
+// warpgroups; each warpgroup owns one 128-edge tile at a time (its 128 TMEM
+// columns, X and H buffers and mbarrier) and runs its own
+// MMA -> epilogue chain, so four tiles are in flight per SM and one
+// warpgroup's epilogue overlaps the others' MMAs.  The gathers of a
+// warpgroup's next tile are issued during its current tile.
 template <int SRC>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(128 * I_WG, 1)
 k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ samples, long long n, EdgeSource es,
             Scales sc, float4* __restrict__ out, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t sm[];
@@ -387,35 +426,36 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
     {
         const uint4* src = reinterpret_cast<const uint4*>(image);
         uint4* dst = reinterpret_cast<uint4*>(sm + S_W);
-        for (int k = tid; k < PK_BYTES / 16; k += 256) dst[k] = src[k];
+        for (int k = tid; k < PK_BYTES / 16; k += blockDim.x) dst[k] = src[k];
     }
     const float* b1 = reinterpret_cast<const float*>(sm + S_W + PK_B);
     const float* b2 = b1 + H;
     const float* b3 = b2 + H;
     const float* b4 = b3 + H;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + I_MISC);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + I_MISC + 8);
-    const uint32_t mb = tc::smem_addr(mbar);
-    if (tid == 0) tc::mbar_init(mb, 1);
-    if (warp == 0) tc::tmem_alloc(tc::smem_addr(tslot), 256);
+    uint64_t* mbars = reinterpret_cast<uint64_t*>(sm + I_MISC);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + I_MISC + 8 * I_WG);
+    const uint32_t mb = tc::smem_addr(mbars + wg);
+    if (row == 0) tc::mbar_init(mb, 1);
+    if (warp == 0) tc::tmem_alloc(tc::smem_addr(tslot), 128 * I_WG);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tb = *tslot;
+    const uint32_t tb = *tslot + 128u * (uint32_t)wg;  // this warpgroup's 128 TMEM columns
     const uint32_t trow = tb + ((uint32_t)((warp & 3) * 32) << 16);
+    uint8_t* xs = sm + I_T + wg * I_TILE_BYTES;
+    uint8_t* hs = xs + TILE * KIN * 2;
     const uint32_t aW1 = tc::smem_addr(sm + S_W + PK_W1), aW2 = tc::smem_addr(sm + S_W + PK_W2);
     const uint32_t aW3 = tc::smem_addr(sm + S_W + PK_W3), aW4 = tc::smem_addr(sm + S_W + PK_W4);
-    const uint32_t aX = tc::smem_addr(sm + I_X), aH = tc::smem_addr(sm + I_H);
-    constexpr uint32_t TD4 = 128;
-    const int c0 = wg * (H / 32), c1 = c0 + H / 32;  // this warpgroup's 16-column chunks
+    const uint32_t aX = tc::smem_addr(xs), aH = tc::smem_addr(hs);
+    const int bar = 1 + wg;
 
     uint32_t phase = 0;
     bool ok = true;
     auto run = [&](auto&& issue) {
         tc::fence_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
+        wg_sync(bar);
+        if (row == 0) {
             tc::fence_after_sync();
             issue();
             tc::commit(mb);
@@ -423,21 +463,54 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
         const bool done = tc::mbar_wait(mb, phase, kWaitLimit);
         phase ^= 1u;
         tc::fence_after_sync();
-        ok = __syncthreads_and(done) != 0;
+        ok = wg_sync_and(bar, done);
     };
     const long long rows = SRC == 0 ? n : es.ne;
     const long long ntiles = (rows + TILE - 1) / TILE;
-    for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+    const long long stride = (long long)gridDim.x * I_WG;
+    long long t = (long long)blockIdx.x * I_WG + wg;
+    // this row's raw inputs, one tile ahead: ids, then the gathers
+    int ni = 0, nj = 0;
+    bool nin = false;
+    double4 pi = make_double4(0, 0, 0, 0), pj = pi, vi = pi, vj = pi;
+    float4 sa = make_float4(0.f, 0.f, 0.f, 0.f), sb = sa, scc = sa;
+    auto load_ids = [&](long long tt) {
+        const long long g = tt * TILE + row;
+        nin = tt < ntiles && g < rows;
+        if (SRC == 1 && nin) {
+            ni = es.ei[g];
+            nj = es.ej[g];
+        }
+    };
+    auto load_raw = [&](long long tt) {
+        if (!nin) return;
+        if (SRC == 0) {
+            const long long g = tt * TILE + row;
+            sa = samples[3 * g];
+            sb = samples[3 * g + 1];
+            scc = samples[3 * g + 2];
+        } else {
+            pi = es.pos[ni];
+            pj = es.pos[nj];
+            vi = es.vel[ni];
+            vj = es.vel[nj];
+        }
+    };
+    load_ids(t);
+    load_raw(t);
+    for (; t < ntiles && ok; t += stride) {
         const long long g = t * TILE + row;
+        const bool in = nin;
         float f[NIN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         bool valid = false;
-        if (wg == 0 && g < rows) {
+        if (in) {
             if (SRC == 0) {
-                float tg[3];
-                valid = sample_features(samples, g, sc, f, tg);
+                const int tt = (int)sb.w;
+                f[0] = sa.x; f[1] = sa.y; f[2] = sa.z;
+                f[3] = sb.x * sc.inv_u; f[4] = sb.y * sc.inv_u; f[5] = sb.z * sc.inv_u;
+                f[6] = sa.w; f[7] = (float)(tt & 3); f[8] = (float)(tt >> 2);
+                valid = scc.w != 0.0f;
             } else {
-                const int i = es.ei[g], j = es.ej[g];
-                const double4 pi = es.pos[i], pj = es.pos[j];
                 double d[3] = {pj.x - pi.x, pj.y - pi.y, pj.z - pi.z};
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
@@ -445,9 +518,8 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
                     else if (d[k] < -es.half_width[k]) d[k] += es.width[k];
                 }
                 const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-                valid = i != j && r2 < es.rv2;
+                valid = ni != nj && r2 < es.rv2;
                 if (valid) {
-                    const double4 vi = es.vel[i], vj = es.vel[j];
                     f[0] = (float)(d[0] * es.inv_l0);
                     f[1] = (float)(d[1] * es.inv_l0);
                     f[2] = (float)(d[2] * es.inv_l0);
@@ -464,39 +536,41 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 #pragma unroll
             for (int k = 0; k < NIN; ++k) f[k] = 0.f;
         }
-        if (wg == 0) store_x(sm + I_X, row, f);
+        store_x(xs, row, f);
+        load_ids(t + stride);
         run([&] { tc::mma_bf16(tb + T_D, tc::desc_k(aX, KIN), tc::desc_k(aW1, KIN), ID_F128, 0u); });
         if (!ok) break;
-        epi_hidden(trow, b1, nullptr, sm + I_H, row, c0, c1);
+        load_raw(t + stride);  // the next tile's ids have arrived during the MMA
+        epi_hidden(trow, b1, nullptr, hs, row);
         run([&] {
             for (int s = 0; s < H / 16; ++s)
                 tc::mma_bf16(tb + T_D, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW2 + 256 * s, H), ID_F128, s > 0);
         });
         if (!ok) break;
-        epi_hidden(trow, b2, nullptr, sm + I_H, row, c0, c1);
+        epi_hidden(trow, b2, nullptr, hs, row);
         run([&] {
             for (int s = 0; s < H / 16; ++s)
                 tc::mma_bf16(tb + T_D, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW3 + 256 * s, H), ID_F128, s > 0);
         });
         if (!ok) break;
-        epi_hidden(trow, b3, nullptr, sm + I_H, row, c0, c1);
-        run([&] {
+        epi_hidden(trow, b3, nullptr, hs, row);
+        run([&] {  // the output layer reuses the first 16 columns
             for (int s = 0; s < H / 16; ++s)
-                tc::mma_bf16(tb + TD4, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW4 + 256 * s, H), ID_F16, s > 0);
+                tc::mma_bf16(tb + T_D, tc::desc_k(aH + 256 * s, H), tc::desc_k(aW4 + 256 * s, H), ID_F16, s > 0);
         });
         if (!ok) break;
         float v[16];
-        tc::tmem_ld16(trow + TD4, v);
-        if (wg == 0 && g < rows) {
+        tc::tmem_ld16(trow + T_D, v);
+        if (in) {
             out[g] = valid ? make_float4((v[0] + b4[0]) * sc.f_scale, (v[1] + b4[1]) * sc.f_scale,
                                          (v[2] + b4[2]) * sc.f_scale, 0.f)
                            : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
-    if (!ok && tid == 0) atomicExch(err, 1);
+    if (!ok && row == 0) atomicExch(err, 1);
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_free(tb, 256);
+    if (warp == 0) tc::tmem_free(*tslot, 128 * I_WG);
 }
 
 // grad[p] = scale * sum of the CTA partials, in CTA order
@@ -684,9 +758,9 @@ int model_adam(Model* m, float lr, float beta1, float beta2, float eps, std::str
 int model_predict(Model* m, const float4* samples, long long n, float4* out, std::string* err) {
     if (n <= 0) return 0;
     const long long ntiles = (n + TILE - 1) / TILE;
-    const int ctas = (int)std::min<long long>(2LL * m->ctas, ntiles);
+    const int ctas = (int)std::min<long long>(m->ctas, (ntiles + I_WG - 1) / I_WG);
     EdgeSource es{};
-    k_mlp_infer<0><<<ctas, 256, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err);
+    k_mlp_infer<0><<<ctas, 128 * I_WG, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err);
     MTRY(cudaGetLastError());
     return check_flag(m, err);
 }
@@ -696,8 +770,8 @@ int model_apply_edges(Model* m, const EdgeSource& src, float4* out, cudaStream_t
     if (launches) *launches = 0;
     if (src.ne <= 0) return 0;
     const long long ntiles = (src.ne + TILE - 1) / TILE;
-    const int ctas = (int)std::min<long long>(2LL * m->ctas, ntiles);
-    k_mlp_infer<1><<<ctas, 256, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err);
+    const int ctas = (int)std::min<long long>(m->ctas, (ntiles + I_WG - 1) / I_WG);
+    k_mlp_infer<1><<<ctas, 128 * I_WG, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err);
     MTRY(cudaGetLastError());
     if (launches) *launches = 1;
     return 0;

@@ -5,7 +5,8 @@ library).
 The network has no reference counterpart (the reference has no learned
 terms); this is a restatement of the same arithmetic in numpy.  `forward` /
 `gradient` with bf16=True round to BF16 where the kernels do (inputs,
-weights, Z = pre-activation, H = SiLU(Z), dY, dZ) and accumulate in FP64 (the
+weights, Z = pre-activation, H = SiLU(Z) at the three rounding points of the
+kernels' packed form, dY, dZ) and accumulate in FP64 (the
 kernels accumulate in FP32 on the tensor cores); with bf16=False everything is
 FP64, which `tests/` checks against finite differences.
 
@@ -79,6 +80,14 @@ def _dsilu(z):
     return sg * (1.0 + z * (1.0 - sg))
 
 
+def _silu_bf16x2(z):
+    """SiLU with the rounding points of the kernels' packed BF16 form (z is
+    already BF16): t = bf16(tanh(z/2)), s = bf16(t/2 + 1/2), h = bf16(z s)."""
+    t = bf16(np.tanh(0.5 * z).astype(np.float32)).astype(np.float64)
+    s = bf16((0.5 * t + 0.5).astype(np.float32)).astype(np.float64)
+    return bf16((z * s).astype(np.float32)).astype(np.float64)
+
+
 def _round(a, on):
     return bf16(a).astype(np.float64) if on else np.asarray(a, np.float64)
 
@@ -94,7 +103,7 @@ def forward(params, samples, velocity_scale=1.0, force_scale=1.0, bf16_on=True):
     h = X
     for W, b in (("W1", "b1"), ("W2", "b2"), ("W3", "b3")):
         z = r((h @ Wb[W].T + P[b]).astype(np.float32) if bf16_on else h @ Wb[W].T + P[b])
-        h = r((_silu(z)).astype(np.float32) if bf16_on else _silu(z))
+        h = _silu_bf16x2(z) if bf16_on else _silu(z)
         Z.append(z)
         Hs.append(h)
     y = (h @ Wb["W4"].T + P["b4"])[:, :NOUT]
