@@ -69,7 +69,7 @@ def measured_bf16_peak() -> float:
 def ncu_traffic(kernel: str, mode: str):
     """DRAM bytes per step of the `kernel` scope on the full-size dam break,
     from the committed ncu summary (profiles/), or None."""
-    tag = kernel + ("_fp32" if mode == "mixed" and kernel == "mix_sweep_b" else "")
+    tag = kernel + ("_fp32" if kernel == "mix_sweep_b" else "")  # one FP32 force sweep in both mixed forms
     p = os.path.join(ROOT, "profiles", "ncu_%s_dam_break_3d.md" % tag)
     if not os.path.exists(p):
         return None

@@ -55,7 +55,7 @@ struct alignas(16) BScene {
     int cc[3], tile[3];
     int has_st, ratio_all_one, uniform_mu, pad0;
     double dmin[3], width[3], inv_width[3], cell_width[3], half_width[3];
-    double dt, shift_thr, grid, inv_grid, vol_d;
+    double dt, shift_thr, grid, inv_grid, vol_d, n0p_d;
     double gravity[3];
     double density[MPH_TYPE_COUNT], bulk_modulus_d[MPH_TYPE_COUNT], bulk_viscosity_d[MPH_TYPE_COUNT];
     float cut2_a, cut2_b, short_r2;
@@ -512,8 +512,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                                 else st_density<true>(sc, ti, tj, r2, rr, dx, dy, dz, sa, cak, g0, g1, g2);
                             }
                     });
-                    const double strain = (double)((sp - cpk) - sc.n0p);
-                    const double div = (double)(sd - cdk);
+                    // the compensated sums keep their low parts; N0p is subtracted in FP64
+                    const double strain = ((double)sp - (double)cpk) - sc.n0p_d;
+                    const double div = (double)sd - (double)cdk;
                     double kappa = sc.bulk_modulus_d[ti];
                     if (strain < 0.0) kappa = 0.0;
                     const double pp = -sc.bulk_viscosity_d[ti] * div + kappa * strain;
@@ -766,6 +767,7 @@ static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& 
     s.vol_over_l0 = (float)c.vol_over_l0;
     s.n0a = (float)c.n0a;
     s.n0p = (float)c.n0p;
+    s.n0p_d = c.n0p;
     s.inv_r2g_rg = (float)(c.rg / c.r2g);
     s.l0 = (float)c.l0;
 }

@@ -16,6 +16,7 @@
 // Quantities the reference computes for output only (DensityA without surface
 // tension, wall forces) are computed when the state is read back.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -28,20 +29,9 @@ namespace {
 
 constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 
-// Resident 128-thread blocks per SM the force-sweep kernels are compiled for
-// (register cap 65536 / (128 * blocks)), and pairs of the long-range loop whose
-// gathers are issued together; set by measurement on the full dam break.  The
-// FP64-core form runs the sweep as a short-range and a long-range kernel, the
-// FP32 form as one fused kernel.
-#ifndef MPH_MIXB_MINB_SHORT
-#define MPH_MIXB_MINB_SHORT 8
-#endif
-#ifndef MPH_MIXB_MINB_LONG
-#define MPH_MIXB_MINB_LONG 8
-#endif
-#ifndef MPH_MIXB_BATCH
-#define MPH_MIXB_BATCH 3
-#endif
+// Resident 128-thread blocks per SM the force sweep is compiled for (register
+// cap 65536 / (128 * blocks)), and pairs of its long-range loop whose gathers
+// are issued together; set by measurement on the full dam break.
 #ifndef MPH_MIXB_MINB_FUSED
 #define MPH_MIXB_MINB_FUSED 8
 #endif
@@ -444,8 +434,10 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
         strain = spd - m.n0p_d;
         div = sdd;
     } else {
-        strain = (double)((sp - cpk) - m.n0p);
-        div = (double)(sd - cdk);
+        // the compensated sum keeps its low part: N0p is subtracted in FP64
+        // (the strain is a small difference of two numbers near N0p)
+        strain = ((double)sp - (double)cpk) - m.n0p_d;
+        div = (double)sd - (double)cdk;
     }
     double kappa = c.bulk_modulus[ti];
     if (strain < 0.0) kappa = 0.0;
@@ -465,31 +457,27 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
     div_out[i] = div;
 }
 
-// Sweep B for fluid particles (WALLS: for the wall particles, output only).
-// The short part of the list: exact displacement, PressureP + ViscosityV (+ the
-// surface-tension terms), Kahan sums (or the FP64 core).  The long part: the hi
-// displacement, ViscosityV (+ surface tension), plain FP32 sum.  Then gravity
-// and the FP64 velocity update (main.cpp:1908-2010).
-// PART 2 does both in one pass.  PART 0 (short part, stores the partial force)
-// and PART 1 (long part, adds it) are the same sweep as two launches, so each
-// gets its own register budget; the sum order is unchanged:
-// ((short FP32 - compensation) + FP64 core) + long.
-template <bool ST, bool RATIO, bool WALLS, bool S64, int PART>
-__global__ void __launch_bounds__(128, PART == 0   ? MPH_MIXB_MINB_SHORT
-                                       : PART == 1 ? MPH_MIXB_MINB_LONG
-                                                   : MPH_MIXB_MINB_FUSED)
+// Sweep B for fluid particles (WALLS: for the wall particles, output only),
+// FP32 in both mixed forms (the FP64 density sweep of MPH_MODE_MIXED_P64 sets
+// the pressures this sweep reads).  The short part of the list: exact
+// displacement, PressureP + ViscosityV (+ the surface-tension terms), Kahan
+// sums.  The long part: the hi displacement, ViscosityV (+ surface tension),
+// plain FP32 sum.  Then gravity and the FP64 velocity update
+// (main.cpp:1908-2010).
+template <bool ST, bool RATIO, bool WALLS>
+__global__ void __launch_bounds__(128, MPH_MIXB_MINB_FUSED)
 k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ p32,
         const float4* __restrict__ p32lo, const float4* __restrict__ pv, const float4* __restrict__ gca,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
         const double4* __restrict__ vel, double4* __restrict__ vel_out, double4* __restrict__ force,
-        StepScalars* __restrict__ scal, const double4* __restrict__ pos64, const double4* __restrict__ press64) {
+        StepScalars* __restrict__ scal) {
     __shared__ SharedTables tb;
     load_tables(m, tb);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m.n) return;
     const int nf = cellstart[c.tot];
     if (WALLS ? i < nf : i >= nf) {
-        if (!WALLS && PART != 0) vel_out[i] = vel[i];
+        if (!WALLS) vel_out[i] = vel[i];
         return;
     }
     const float4 pi = p32[i];
@@ -504,49 +492,9 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     const float mu_u = tb.mu[ti * 4 + ti];
     float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // short part, Kahan
     float gx = 0.f, gy = 0.f, gz = 0.f;                                 // long part
-    double hx = 0.0, hy = 0.0, hz = 0.0;                                // short part, FP64 core
     const unsigned* lp = list + i;
     int k = 0;
-    if (PART == 1) {
-        k = ns;
-        lp += (size_t)ns * n;
-    } else if (S64) {
-        const double4 pid = pos64[i];
-        const double4 vid = press64[i];  // {v, PressureP}
-        const double mu_d = c.visc_mu[ti][ti];
-        for (; k < ns; ++k, lp += n) {
-            const unsigned e = __ldg(lp);
-            const int j = (int)(e >> kCodeBits);
-            double dx, dy, dz;
-            disp64(c, pid, pos64[j], dx, dy, dz);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (!(r2 < c.rv2 || r2 < c.rp2 || (ST && (r2 < c.ra2 || r2 < c.rg2)))) continue;
-            const double y = rsqrt64(r2);
-            const double r = r2 * y;
-            const double4 vj = press64[j];
-            const int tj = c.ratio_all_one && m.uniform_mu ? ti : __float_as_int(p32[j].w);
-            double sdd = 0.0;
-            if (r2 < c.rp2) sdd += (vid.w + vj.w) * (m.p_a_d + m.p_b_d * r) * y;
-            if (r2 < c.rv2) {
-                const double mu = m.uniform_mu ? mu_d : c.visc_mu[ti][tj];
-                const double ud = (vj.x - vid.x) * dx + (vj.y - vid.y) * dy + (vj.z - vid.z) * dz;
-                sdd += mu * ud * (m.v_a_d + m.v_b_d * r) * (y * y * y);
-            }
-            if (ST) {
-                float3 t = make_float3(0.f, 0.f, 0.f);
-                const float sf = st_terms<RATIO>(m, ti, tj, (float)r2, (float)r, (float)y, (float)dx, (float)dy,
-                                                 (float)dz, gi, gca[j], ai, t);
-                sdd += sf;
-                hx += t.x;
-                hy += t.y;
-                hz += t.z;
-            }
-            hx += sdd * dx;
-            hy += sdd * dy;
-            hz += sdd * dz;
-        }
-    }
-    if (PART != 1) for (; k < ns; ++k, lp += n) {
+    for (; k < ns; ++k, lp += n) {
         const unsigned e = __ldg(lp);
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         float4 pj, vj;
@@ -574,13 +522,8 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         kahan_add(fy, cy, fmaf(s, dy, t.y));
         kahan_add(fz, cz, fmaf(s, dz, t.z));
     }
-    if (PART == 0) {
-        force[i] = make_double4(((double)fx - (double)cx) + hx, ((double)fy - (double)cy) + hy,
-                                ((double)fz - (double)cz) + hz, 0.0);
-        return;
-    }
-    // long part: MPH_MIXB_BATCH pairs per iteration, their gathers issued
-    // together so a thread keeps 2 * MPH_MIXB_BATCH independent loads in flight
+    // long part: MPH_MIXB_BATCH_FUSED pairs per iteration, their gathers issued
+    // together so a thread keeps that many independent loads in flight
     auto long_pair = [&](unsigned e, const float4& pj, const float4& vj) {
         const int code = (int)(e & 31u);
         const float4 dh = tb.dhi[code];
@@ -608,16 +551,14 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         gy = fmaf(s, dy, gy);
         gz = fmaf(s, dz, gz);
     };
-    constexpr int U = PART == 2 ? MPH_MIXB_BATCH_FUSED : MPH_MIXB_BATCH;
+    constexpr int U = MPH_MIXB_BATCH_FUSED;
     for (; k + U <= na; k += U, lp += U * n) {
         unsigned e[U];
         float4 pj[U], vj[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) e[u] = __ldg(lp + (size_t)u * n);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            ldg_pv(pv, (int)(e[u] >> kCodeBits), pj[u], vj[u]);
-        }
+        for (int u = 0; u < U; ++u) ldg_pv(pv, (int)(e[u] >> kCodeBits), pj[u], vj[u]);
 #pragma unroll
         for (int u = 0; u < U; ++u) long_pair(e[u], pj[u], vj[u]);
     }
@@ -627,16 +568,9 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         ldg_pv(pv, (int)(e >> kCodeBits), pj, vj);
         long_pair(e, pj, vj);
     }
-    double4 fs;
-    if (PART == 1) {
-        fs = force[i];
-    } else {
-        fs = make_double4(((double)fx - (double)cx) + hx, ((double)fy - (double)cy) + hy,
-                          ((double)fz - (double)cz) + hz, 0.0);
-    }
-    double F0 = fs.x + (double)gx;
-    double F1 = fs.y + (double)gy;
-    double F2 = fs.z + (double)gz;
+    double F0 = ((double)fx - (double)cx) + (double)gx;
+    double F1 = ((double)fy - (double)cy) + (double)gy;
+    double F2 = ((double)fz - (double)cz) + (double)gz;
     if (WALLS) {
         force[i] = make_double4(F0, F1, F2, 0.0);
         return;
@@ -815,30 +749,22 @@ template <bool WALLS>
 static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     const int nb = blocks(c.n, 128);
     double4* vout = WALLS ? nullptr : d.vel[1 - d.vcur];
-#define MIX_B1(ST, RATIO, S64, PART)                                                                        \
-    k_mix_b<ST, RATIO, WALLS, S64, PART><<<nb, 128, 0, s>>>(                                              \
-        m->mc, c, d.cellstart, m->p32, m->p32lo, m->pv, m->gca, m->list, m->cnt_short, m->cnt_all,     \
-        d.vel[d.vcur], vout, d.force, d.scal, d.pos[d.cur], d.press)
-#define MIX_B2(ST, RATIO)             \
-    if (m->s64) {                     \
-        MIX_B1(ST, RATIO, true, 0);   \
-        MIX_B1(ST, RATIO, true, 1);   \
-    } else {                          \
-        MIX_B1(ST, RATIO, false, 2);  \
-    }
+#define MIX_B1(ST, RATIO)                                                                                   \
+    k_mix_b<ST, RATIO, WALLS><<<nb, 128, 0, s>>>(m->mc, c, d.cellstart, m->p32, m->p32lo, m->pv, m->gca,   \
+                                                 m->list, m->cnt_short, m->cnt_all, d.vel[d.vcur], vout,   \
+                                                 d.force, d.scal)
     if (m->mc.has_st) {
-        if (m->mc.ratio_all_one) { MIX_B2(true, false); } else { MIX_B2(true, true); }
+        if (m->mc.ratio_all_one) { MIX_B1(true, false); } else { MIX_B1(true, true); }
     } else {
-        if (m->mc.ratio_all_one) { MIX_B2(false, false); } else { MIX_B2(false, true); }
+        if (m->mc.ratio_all_one) { MIX_B1(false, false); } else { MIX_B1(false, true); }
     }
-#undef MIX_B2
 #undef MIX_B1
 }
 
 int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     launch_b<false>(m, c, d, s);
     m->exported = false;
-    return m->s64 ? 2 : 1;
+    return 1;
 }
 
 void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
@@ -995,7 +921,7 @@ int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, s
         }
         launch_b<true>(m, c, d, s);  // wall forces
         k_mix_counts<<<blocks(c.n, 256), 256, 0, s>>>(c.n, m->cnt_all, d.cellstart, c.tot, d.ncount);
-        nl += (m->s64 ? 2 : 1) + 1;
+        nl += 2;
         MTRY(cudaGetLastError());
         m->exported = true;
     }

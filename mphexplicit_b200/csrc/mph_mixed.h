@@ -11,8 +11,9 @@ namespace mph {
 struct MixedState;
 
 // Allocate, sort, build the table and run the start-up density sweep.
-// fp64_pressure: the short-range pressure pairs (DensityP, DivergenceP,
-// PressureP force) in FP64, the rest in FP32 (MPH_MODE_MIXED_P64).
+// fp64_pressure: the density sweep's short-range pairs (DensityP,
+// DivergenceP, hence the PressureP values) in FP64, the rest in FP32
+// (MPH_MODE_MIXED_P64).
 int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, DevFP64& d, bool fp64_pressure,
                  cudaStream_t s, std::string* err);
 // Convection/wall/periodic + displacement maximum + FP32 copies (1 launch).
@@ -21,8 +22,8 @@ void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
 int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);
 // Density sweep (1 launch); advance_wall moves the wall centres one step.
 void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wall, cudaStream_t s);
-// Force sweep + FP64 velocity update into d.vel[1 - d.vcur]; returns the
-// number of launches (2 with the FP64 pressure core, else 1).
+// Force sweep (FP32 pairs) + FP64 velocity update into d.vel[1 - d.vcur];
+// returns the number of launches (1).
 int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
 // Fill the output-only fields (DensityA, wall forces, neighbour counts).
 int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);

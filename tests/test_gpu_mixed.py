@@ -2,7 +2,7 @@
 
 MPH_MODE_MIXED: every pair term in FP32 (cell-relative, exact FP32
 displacements, Kahan sums), FP64 integration.  MPH_MODE_MIXED_P64: the same with
-the short-range pressure pairs (DensityP, DivergenceP, PressureP force) in FP64.
+the density sweep's pressure pairs (DensityP, DivergenceP) in FP64.
 Errors are relative L2 norms of the fluid velocity against the FP64 form,
 matched by ParticleIndex; the tolerances below are the contract of each form.
 """
