@@ -41,6 +41,7 @@ constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 
 struct MixConst {
     int n, tot, dim, has_st, ratio_all_one, uniform_mu;
+    int cap_s;                         // table rows of the short part; the long part follows
     int cc[3], range[3];
     double grid, inv_grid;             // hi-part grid (a power of two, metres)
     float dhi[27][4];                  // cell-origin offset per code: hi part (on the grid)
@@ -95,6 +96,21 @@ __device__ __forceinline__ void rel32(const SimConst& c, const MixConst& m, cons
     }
     hi = make_float4(h3[0], h3[1], h3[2], __int_as_float((int)p.w));
     lo = make_float4(l3[0], l3[1], l3[2], 0.0f);
+}
+
+// The neighbour table holds entries in rows of four: entries 4r..4r+3 of
+// particle i are one uint4 at row r, column i (tab[r * n + i]), so a lane
+// writes 16 bytes at a time when the table is built and the lanes of a warp
+// read consecutive uint4 when it is swept.  Visits entries [0, cnt) in order.
+template <class F>
+__device__ __forceinline__ void for_entries(const uint4* __restrict__ tab, size_t n, int cnt, F&& f) {
+    for (int k = 0; k < cnt; k += 4) {
+        const uint4 q = __ldg(tab + (size_t)(k >> 2) * n);
+        f(q.x);
+        if (k + 1 < cnt) f(q.y);
+        if (k + 2 < cnt) f(q.z);
+        if (k + 3 < cnt) f(q.w);
+    }
 }
 
 // ---- counting sort by cell ------------------------------------------------
@@ -184,12 +200,13 @@ __global__ void k_mix_home(SimConst c, MixConst m, const double4* __restrict__ p
 }
 
 // Neighbour table: for particle i, the 3^D stencil (same visiting order as
-// main.cpp:1356-1392), entries (j << 5 | code); pass 0 keeps pairs within
-// RP+margin, pass 1 the rest within MaxRadius+margin.  Self is excluded.
+// main.cpp:1356-1392), entries (j << 5 | code), in one pass: pairs within
+// RP+margin go to rows [0, cap_s), the rest within MaxRadius+margin to rows
+// [cap_s, cap_s + cap_l), each part in stencil order.  Self is excluded.
 // Walls without a fluid neighbour get no list (their pressure is never used).
 __global__ void __launch_bounds__(128)
 k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __restrict__ keys,
-           const int* __restrict__ cellstart, unsigned* __restrict__ list, int cap, int* __restrict__ cnt_short,
+           const int* __restrict__ cellstart, unsigned* __restrict__ list, int cap_l, int* __restrict__ cnt_short,
            int* __restrict__ cnt_all, StepScalars* __restrict__ scal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -208,40 +225,57 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
     const int nf = cellstart[c.tot];
     const bool is_wall = i >= nf;
     const size_t n = (size_t)c.n;
-    int cnt = 0, cshort = 0;
+    const int cap_s = m.cap_s;
+    uint4* const ls = reinterpret_cast<uint4*>(list) + i;
+    uint4* const ll = reinterpret_cast<uint4*>(list) + (size_t)(cap_s >> 2) * n + i;
+    int cs = 0, cl = 0;
+    unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, l0 = 0, l1 = 0, l2 = 0, l3 = 0;  // rows being filled
+    auto push = [n](unsigned e, int& cnt, int cap, uint4* row0, unsigned& b0, unsigned& b1, unsigned& b2,
+                    unsigned& b3) {
+        switch (cnt & 3) {
+            case 0: b0 = e; break;
+            case 1: b1 = e; break;
+            case 2: b2 = e; break;
+            default:
+                b3 = e;
+                if (cnt < cap) row0[(size_t)(cnt >> 2) * n] = make_uint4(b0, b1, b2, b3);
+        }
+        ++cnt;
+    };
     bool any_fluid = !is_wall;  // a wall needs a list only if a fluid particle is within reach
-    for (int pass = 0; pass < 2; ++pass) {
-        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
-                    const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
-                    const int cell = jc[0][ax] * c.cc[1] * c.cc[2] + jc[1][ay] * c.cc[2] + jc[2][az];
-                    const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
-                    const float ox = m.dhi[code][0], oy = m.dhi[code][1], oz = m.dhi[code][2];
-                    for (int kind = 0; kind < 2; ++kind) {
-                        const int off = kind ? c.tot : 0;
-                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
-                        for (int j = b; j < e; ++j) {
-                            if (j == i) continue;
-                            const float4 pj = p32[j];
-                            const float dx = (pj.x - pi.x) + ox, dy = (pj.y - pi.y) + oy, dz = (pj.z - pi.z) + oz;
-                            const float r2 = dx * dx + dy * dy + dz * dz;
-                            const bool near = r2 < m.short_r2;
-                            if (r2 < m.list_r2 && (pass == 0 ? near : !near)) {
-                                if (kind == 0) any_fluid = true;
-                                if (cnt < cap) list[(size_t)cnt * n + i] = ((unsigned)j << kCodeBits) | (unsigned)code;
-                                ++cnt;
-                            }
+    for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+        for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+            for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
+                const int cell = jc[0][ax] * c.cc[1] * c.cc[2] + jc[1][ay] * c.cc[2] + jc[2][az];
+                const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
+                const float ox = m.dhi[code][0], oy = m.dhi[code][1], oz = m.dhi[code][2];
+                for (int kind = 0; kind < 2; ++kind) {
+                    const int off = kind ? c.tot : 0;
+                    const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                    for (int j = b; j < e; ++j) {
+                        if (j == i) continue;
+                        const float4 pj = p32[j];
+                        const float dx = (pj.x - pi.x) + ox, dy = (pj.y - pi.y) + oy, dz = (pj.z - pi.z) + oz;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 < m.list_r2) {
+                            if (kind == 0) any_fluid = true;
+                            const unsigned entry = ((unsigned)j << kCodeBits) | (unsigned)code;
+                            if (r2 < m.short_r2) push(entry, cs, cap_s, ls, s0, s1, s2, s3);
+                            else push(entry, cl, cap_l, ll, l0, l1, l2, l3);
                         }
                     }
                 }
-        if (pass == 0) cshort = cnt;
-    }
-    if (is_wall && !any_fluid) cnt = cshort = 0;
-    cnt_short[i] = cshort;
-    cnt_all[i] = cnt;
-    atomicMax(&scal->max_neighbors, cnt);
-    if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+            }
+    if ((cs & 3) != 0 && cs < cap_s) ls[(size_t)(cs >> 2) * n] = make_uint4(s0, s1, s2, s3);
+    if ((cl & 3) != 0 && cl < cap_l) ll[(size_t)(cl >> 2) * n] = make_uint4(l0, l1, l2, l3);
+    if (is_wall && !any_fluid) cs = cl = 0;
+    cnt_short[i] = cs;
+    cnt_all[i] = cs + cl;
+    atomicMax(&scal->max_neighbors, cs + cl);
+    atomicMax(&scal->max_short, cs);
+    atomicMax(&scal->max_long, cl);
+    if (cs > cap_s || cl > cap_l) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
 }
 
 // ---- per step -----------------------------------------------------------------
@@ -377,10 +411,8 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
     float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
     double spd = 0.0, sdd = 0.0;
     float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
-    const unsigned* lp = list + i;
-    int k = 0;
-    for (; k < ns; ++k, lp += n) {
-        const unsigned e = __ldg(lp);
+    const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
+    for_entries(tab, n, ns, [&](unsigned e) {
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         const float4 pj = p32[j];
         const float4 dh = tb.dhi[code];
@@ -419,15 +451,16 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
             kahan_add(sd, cdk, -ue * dw);
         }
         if (ST) st_density<RATIO>(m, ti, __float_as_int(pj.w), r2, r, dx, dy, dz, sa, cak, g0, g1, g2);
-    }
-    for (; k < na; ++k, lp += n) {  // surface tension only: the long part
-        const unsigned e = __ldg(lp);
-        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
-        const float4 pj = p32[j];
-        const float4 dh = tb.dhi[code];
-        const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        st_density<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rsqrtf(r2), dx, dy, dz, sa, cak, g0, g1, g2);
+    });
+    if (ST) {  // surface tension only: the long part
+        for_entries(tab + (size_t)(m.cap_s >> 2) * n, n, na - ns, [&](unsigned e) {
+            const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+            const float4 pj = p32[j];
+            const float4 dh = tb.dhi[code];
+            const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            st_density<RATIO>(m, ti, __float_as_int(pj.w), r2, r2 * rsqrtf(r2), dx, dy, dz, sa, cak, g0, g1, g2);
+        });
     }
     double strain, div;
     if (S64) {
@@ -492,10 +525,8 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     const float mu_u = tb.mu[ti * 4 + ti];
     float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // short part, Kahan
     float gx = 0.f, gy = 0.f, gz = 0.f;                                 // long part
-    const unsigned* lp = list + i;
-    int k = 0;
-    for (; k < ns; ++k, lp += n) {
-        const unsigned e = __ldg(lp);
+    const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
+    for_entries(tab, n, ns, [&](unsigned e) {
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         float4 pj, vj;
         ldg_pv(pv, j, pj, vj);
@@ -505,7 +536,7 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         const float dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
         const float dz = ((pj.z - pi.z) + dh.z) + ((lj.z - li.z) + dl.z);
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 < m.rv2 || r2 < m.rp2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) continue;
+        if (!(r2 < m.rv2 || r2 < m.rp2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) return;
         const float rinv = rsqrt_nr(r2);
         const float r = r2 * rinv;
         const int tj = __float_as_int(pj.w);
@@ -521,9 +552,9 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         kahan_add(fx, cx, fmaf(s, dx, t.x));
         kahan_add(fy, cy, fmaf(s, dy, t.y));
         kahan_add(fz, cz, fmaf(s, dz, t.z));
-    }
-    // long part: MPH_MIXB_BATCH_FUSED pairs per iteration, their gathers issued
-    // together so a thread keeps that many independent loads in flight
+    });
+    // long part: a row of four pairs per iteration, their gathers issued
+    // together so a thread keeps four independent loads in flight
     auto long_pair = [&](unsigned e, const float4& pj, const float4& vj) {
         const int code = (int)(e & 31u);
         const float4 dh = tb.dhi[code];
@@ -551,22 +582,18 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         gy = fmaf(s, dy, gy);
         gz = fmaf(s, dz, gz);
     };
-    constexpr int U = MPH_MIXB_BATCH_FUSED;
-    for (; k + U <= na; k += U, lp += U * n) {
-        unsigned e[U];
-        float4 pj[U], vj[U];
+    const uint4* tl = tab + (size_t)(m.cap_s >> 2) * n;
+    const int nl = na - ns;
+    for (int k = 0; k < nl; k += 4) {
+        const uint4 q = __ldg(tl + (size_t)(k >> 2) * n);
+        const unsigned e[4] = {q.x, q.y, q.z, q.w};
+        float4 pj[4], vj[4];
 #pragma unroll
-        for (int u = 0; u < U; ++u) e[u] = __ldg(lp + (size_t)u * n);
+        for (int u = 0; u < 4; ++u)
+            if (k + u < nl) ldg_pv(pv, (int)(e[u] >> kCodeBits), pj[u], vj[u]);
 #pragma unroll
-        for (int u = 0; u < U; ++u) ldg_pv(pv, (int)(e[u] >> kCodeBits), pj[u], vj[u]);
-#pragma unroll
-        for (int u = 0; u < U; ++u) long_pair(e[u], pj[u], vj[u]);
-    }
-    for (; k < na; ++k, lp += n) {
-        const unsigned e = __ldg(lp);
-        float4 pj, vj;
-        ldg_pv(pv, (int)(e >> kCodeBits), pj, vj);
-        long_pair(e, pj, vj);
+        for (int u = 0; u < 4; ++u)
+            if (k + u < nl) long_pair(e[u], pj[u], vj[u]);
     }
     double F0 = ((double)fx - (double)cx) + (double)gx;
     double F1 = ((double)fy - (double)cy) + (double)gy;
@@ -590,7 +617,8 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
 
 // DensityA over the whole list (output only, without surface tension).
 __global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, const unsigned* __restrict__ list,
-                                const int* __restrict__ cnt_all, double* __restrict__ dens_a_out) {
+                                const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
+                                double* __restrict__ dens_a_out) {
     __shared__ SharedTables tb;
     load_tables(m, tb);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -599,9 +627,9 @@ __global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, cons
     const int ti = __float_as_int(pi.w);
     const size_t n = (size_t)m.n;
     float sa = 0.f, ck = 0.f;
-    const unsigned* lp = list + i;
-    for (int k = 0; k < cnt_all[i]; ++k, lp += n) {
-        const unsigned e = *lp;
+    const int ns = cnt_short[i], na = cnt_all[i];
+    const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
+    auto visit = [&](unsigned e) {
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         const float4 pj = p32[j];
         const float4 dh = tb.dhi[code];
@@ -613,7 +641,9 @@ __global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, cons
             const float ratio = m.ratio_all_one ? 1.0f : m.ratio[ti][__float_as_int(pj.w)];
             kahan_add(sa, ck, ratio * m.ca * q * (1.0f - q) * (1.0f - q));
         }
-    }
+    };
+    for_entries(tab, n, ns, visit);
+    for_entries(tab + (size_t)(m.cap_s >> 2) * n, n, na - ns, visit);
     dens_a_out[i] = sa - ck;
 }
 
@@ -645,7 +675,9 @@ struct MixedState {
     float4* pv = nullptr;  // [2n]: {p32, (v, PressureP)} per particle, written by sweep A
     float4* gca = nullptr;
     unsigned* list = nullptr;
-    int cap = 0;
+    int cap = 0;          // cap_s + cap_l rows
+    int cap_l = 0;        // rows of the long part (mc.cap_s: the short part)
+    int max_short = 0, max_long = 0;
     int* cnt_short = nullptr;
     int* cnt_all = nullptr;
     StepScalars* h_scal = nullptr;
@@ -676,13 +708,15 @@ static cudaError_t malloc_n(T** p, size_t n) {
     return cudaMalloc((void**)p, (n ? n : 1) * sizeof(T));
 }
 
-static int grow_list(MixedState* m, int need, int n, std::string* err) {
-    int cap = ((int)(need * 1.15) + 8 + 31) / 32 * 32;
+static int grow_list(MixedState* m, int need_s, int need_l, int n, std::string* err) {
+    const int cs = ((int)(need_s * 1.15) + 8 + 7) / 8 * 8, cl = ((int)(need_l * 1.15) + 8 + 7) / 8 * 8;
     if (m->list) cudaFree(m->list);
     m->list = nullptr;
-    m->cap = 0;
-    MTRY(malloc_n(&m->list, (size_t)cap * (size_t)n));
-    m->cap = cap;
+    m->cap = m->cap_l = m->mc.cap_s = 0;
+    MTRY(malloc_n(&m->list, (size_t)(cs + cl) * (size_t)n));
+    m->mc.cap_s = cs;
+    m->cap_l = cl;
+    m->cap = cs + cl;
     return MPH_OK;
 }
 
@@ -705,19 +739,22 @@ int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, 
     nl += 6;
     for (int attempt = 0; attempt < 3; ++attempt) {
         MTRY(cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), s));
-        k_mix_list<<<blocks(n, 128), 128, 0, s>>>(c, m->mc, m->p32, d.keys, d.cellstart, m->list, m->cap,
+        MTRY(cudaMemsetAsync(&d.scal->max_short, 0, 2 * sizeof(int), s));
+        k_mix_list<<<blocks(n, 128), 128, 0, s>>>(c, m->mc, m->p32, d.keys, d.cellstart, m->list, m->cap_l,
                                                   m->cnt_short, m->cnt_all, d.scal);
         ++nl;
         MTRY(cudaGetLastError());
         MTRY(cudaMemcpyAsync(m->h_scal, d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, s));
         MTRY(cudaStreamSynchronize(s));
         m->max_neighbors = m->h_scal->max_neighbors;
-        if (m->max_neighbors <= m->cap) break;
-        const int st = grow_list(m, m->max_neighbors, n, err);
+        m->max_short = m->h_scal->max_short;
+        m->max_long = m->h_scal->max_long;
+        if (m->max_short <= m->mc.cap_s && m->max_long <= m->cap_l) break;
+        const int st = grow_list(m, std::max(m->max_short, m->mc.cap_s), std::max(m->max_long, m->cap_l), n, err);
         if (st != MPH_OK) return st;
     }
     if (launches) *launches = nl;
-    if (m->max_neighbors > m->cap) {
+    if (m->max_short > m->mc.cap_s || m->max_long > m->cap_l) {
         if (err) *err = "mixed neighbour table could not grow";
         return MPH_ERR_CAPACITY;
     }
@@ -885,15 +922,18 @@ int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, De
         delete m;
         return MPH_ERR_NOMEM;
     }
-    // initial table: lattice points within the cut-off, with head room
-    const double ratio = rl / c.l0;
+    // initial table: lattice points within the short and the long cut-off, with head room
+    const double ratio = rl / c.l0, rs_l0 = rs / c.l0;
     const int r = (int)ratio + 1, zr = c.dim == 2 ? 0 : r;
-    int lat = 0;
+    int lat_s = 0, lat_l = 0;
     for (int x = -r; x <= r; ++x)
         for (int y = -r; y <= r; ++y)
-            for (int z = -zr; z <= zr; ++z)
-                if (x * x + y * y + z * z <= ratio * ratio) ++lat;
-    int st = grow_list(m, (int)(lat * 1.1) + 8, c.n, err);
+            for (int z = -zr; z <= zr; ++z) {
+                const double q2 = x * x + y * y + z * z;
+                if (q2 <= rs_l0 * rs_l0) ++lat_s;
+                else if (q2 <= ratio * ratio) ++lat_l;
+            }
+    int st = grow_list(m, (int)(lat_s * 1.1) + 4, (int)(lat_l * 1.1) + 8, c.n, err);
     if (st == MPH_OK) st = mixed_rebuild(m, c, d, s, err, nullptr);
     if (st == MPH_OK) {
         mixed_sweep_a(m, c, d, false, s);
@@ -916,7 +956,8 @@ int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, s
     int nl = 0;
     if (!m->exported) {
         if (!m->mc.has_st) {
-            k_mix_density_a<<<blocks(c.n, 128), 128, 0, s>>>(m->mc, m->p32, m->list, m->cnt_all, d.dens_a);
+            k_mix_density_a<<<blocks(c.n, 128), 128, 0, s>>>(m->mc, m->p32, m->list, m->cnt_short, m->cnt_all,
+                                                               d.dens_a);
             ++nl;
         }
         launch_b<true>(m, c, d, s);  // wall forces

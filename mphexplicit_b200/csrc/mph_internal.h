@@ -54,7 +54,8 @@ struct StepScalars {
     int flags;                           // MPH_DEVFLAG_*
     int max_neighbors;                   // longest list of the last build
     int rebuild;                         // decision of the last move kernel
-    int pad[11];
+    int max_short, max_long;             // longest short / long part (mixed table)
+    int pad[9];
 };
 
 enum : int {
