@@ -13,7 +13,7 @@ value = fluid particles x steps / seconds, summed over ranks (replicas: the
 step does not shard, each rank runs its own scene on its own GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed|mixed_p64] [--only]
-                  [--forms fp64,mixed,mixed_p64,learned,batch]
+                  [--forms fp64,mixed,mixed_p64,learned,batch,two_fluid]
   python bench.py --impl reference ...   # the reference's own CPU step, all host threads
 
 One JSON line on rank 0.
@@ -323,6 +323,54 @@ def measure_batch(args, rank):
     return out
 
 
+def measure_two_fluid(args, rank):
+    """Benchmark config 3: the two-fluid column (200^3 fluid, l0 = 0.0025 m,
+    lower half type 0 at rho 500, upper half type 1 at rho 1000, interface
+    displaced by a seeded sum of 4 cosine modes of amplitude 2 l0, 2-layer
+    type-2/3 walls, mu 0.01, sigma 0.05, dt 1e-5 s): both mixed forms timed over
+    `two_fluid_steps` steps, each with its velocity error against the FP64 form
+    over the same steps."""
+    import torch
+    import mphexplicit_b200 as M
+    from mphexplicit_b200 import scenes
+    n = args.two_fluid_n
+    sc = scenes.two_fluid_column(n=n, seed=rank)
+    out = {"workload": "two_fluid_column %d^3 fluid, 2 wall layers: %d particles (%d fluid)" % (n, sc.n, sc.n_fluid)}
+    res = {}
+    for mode in ("mixed", "mixed_p64", "fp64"):
+        s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode=mode)
+        s.step(3)
+        s.synchronize()
+        stream = torch.cuda.ExternalStream(s.stream_handle)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.profile(True)
+        ev0.record(stream)
+        s.step(args.two_fluid_steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        prof = s.profile_read()
+        info = s.info()
+        st = s.state()
+        s.close()
+        order = np.argsort(st["particle_index"], kind="stable")
+        res[mode] = {"ms": ms, "vel": st["vel"][order], "fluid": st["type"][order] < 2, "prof": prof,
+                     "rebuilds": info["rebuild_count"]}
+    steps = args.two_fluid_steps
+    f = res["fp64"]
+    fl = f["fluid"]
+    out.update({"steps": steps, "error_steps": 3 + steps, "fp64_ms_per_step": f["ms"] / steps})
+    for mode in ("mixed", "mixed_p64"):
+        r = res[mode]
+        out[mode] = {"value": sc.n_fluid * steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / steps,
+                     "speedup_vs_fp64": f["ms"] / r["ms"], "rebuilds": r["rebuilds"],
+                     "rel_l2_vel_vs_fp64": float(np.linalg.norm(r["vel"][fl] - f["vel"][fl]) /
+                                                 np.linalg.norm(f["vel"][fl])),
+                     "kernels_ms_per_step": {k: v[1] / steps for k, v in r["prof"].items()}}
+    out["value"] = out["mixed"]["value"]
+    return out
+
+
 def make_scene(args, rank):
     from mphexplicit_b200 import scenes
     if args.scene == "dam":
@@ -473,13 +521,15 @@ def main():
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch",
+    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch,two_fluid",
                     help="forms to measure (comma list); the headline --mode must be among them for a full line")
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
     ap.add_argument("--learn-epochs", type=int, default=4)
     ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--two-fluid-n", type=int, default=200, help="fluid particles per axis of the two-fluid column")
+    ap.add_argument("--two-fluid-steps", type=int, default=50)
     ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
     ap.add_argument("--batch-cpu-scenes", type=int, default=16)
     ap.add_argument("--batch-cpu-steps", type=int, default=200)
@@ -529,6 +579,8 @@ def main():
         forms["learned"] = measure_learned(args, rank)
     if "batch" in wanted:
         forms["batch"] = measure_batch(args, rank)
+    if "two_fluid" in wanted:
+        forms["two_fluid"] = measure_two_fluid(args, rank)
     if args.mode not in res:  # a run of the extra forms alone (profiling)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "unit": UNIT, "n_gpus": world, "forms": forms}), flush=True)
