@@ -374,14 +374,18 @@ int mph_batch_synchronize(mph_batch* b);
 /* Positions and velocities of every scene in its input order (layout of
  * mph_batch_create's xyz / vel). */
 int mph_batch_get_state(mph_batch* b, double* xyz, double* vel);
-/* Cell tile (tz ignored in 2-D) and CTA size of the sweeps. */
-int mph_batch_set_tiles(mph_batch* b, int tx, int ty, int tz, int threads);
+/* Cell tile (tz ignored in 2-D), CTA size of the sweeps, and the resident CTAs
+ * per SM their staging capacity is sized for (0: keep the current value). */
+int mph_batch_set_tiles(mph_batch* b, int tx, int ty, int tz, int threads, int ctas_per_sm);
 typedef struct mph_batch_trial {
     int tile[3];
     int threads;
+    int ctas_per_sm;   /* resident CTAs per SM the staging capacity is sized for */
+    int capacity;      /* particles a CTA stages (tile + halo) before splitting  */
     double ms_per_step;
 } mph_batch_trial;
-/* Time every candidate tile shape and CTA size on the batch itself for about
+/* Time every candidate tile shape, CTA size and staging capacity (sized for 2
+ * to 4 resident CTAs per SM in 2-D, 1 or 2 in 3-D) on the batch itself for about
  * `steps` steps each, keep the fastest, and put the batch state back as it
  * was: the simulation does not advance.  trials[capacity] receives the
  * timings (may be NULL), *count the number of candidates timed. */
@@ -389,7 +393,7 @@ int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* trials, int cap
 typedef struct mph_batch_info {
     int dim, scenes, particles, fluid_particles;
     int tile[3];
-    int threads, items, capacity, grid_a, grid_b, graph_steps;
+    int threads, ctas_per_sm, items, capacity, grid_a, grid_b, graph_steps;
     long long steps;            /* steps taken                                   */
     long long scene_rebuilds;   /* per-scene cell sorts since creation            */
     long long tile_splits;      /* tiles split because their halo did not fit     */

@@ -137,14 +137,16 @@ class LearnedInfo(C.Structure):
 class BatchTrial(C.Structure):
     """mph_batch_trial: one candidate of the batch autotuner."""
 
-    _fields_ = [("tile", C.c_int * 3), ("threads", C.c_int), ("ms_per_step", C.c_double)]
+    _fields_ = [("tile", C.c_int * 3), ("threads", C.c_int), ("ctas_per_sm", C.c_int), ("capacity", C.c_int),
+                ("ms_per_step", C.c_double)]
 
 
 class BatchInfo(C.Structure):
     """mph_batch_info: shape and counters of a batch."""
 
     _fields_ = [("dim", C.c_int), ("scenes", C.c_int), ("particles", C.c_int), ("fluid_particles", C.c_int),
-                ("tile", C.c_int * 3), ("threads", C.c_int), ("items", C.c_int), ("capacity", C.c_int),
+                ("tile", C.c_int * 3), ("threads", C.c_int), ("ctas_per_sm", C.c_int), ("items", C.c_int),
+                ("capacity", C.c_int),
                 ("grid_a", C.c_int), ("grid_b", C.c_int), ("graph_steps", C.c_int), ("steps", C.c_longlong),
                 ("scene_rebuilds", C.c_longlong), ("tile_splits", C.c_longlong), ("launches", C.c_longlong)]
 
@@ -209,7 +211,7 @@ SIGNATURES = {
     "mph_batch_step": (_I, [_P, _I]),
     "mph_batch_synchronize": (_I, [_P]),
     "mph_batch_get_state": (_I, [_P, _dp, _dp]),
-    "mph_batch_set_tiles": (_I, [_P, _I, _I, _I, _I]),
+    "mph_batch_set_tiles": (_I, [_P, _I, _I, _I, _I, _I]),
     "mph_batch_autotune": (_I, [_P, _I, C.POINTER(BatchTrial), _I, _ip]),
     "mph_batch_get_info": (_I, [_P, C.POINTER(BatchInfo)]),
     "mph_batch_stream": (_P, [_P]),

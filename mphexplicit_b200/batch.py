@@ -73,15 +73,17 @@ class Batch:
     def synchronize(self) -> None:
         _bcheck(self._lib.mph_batch_synchronize(self.handle), self.handle)
 
-    def set_tiles(self, tx: int, ty: int, tz: int = 1, threads: int = 256) -> None:
-        _bcheck(self._lib.mph_batch_set_tiles(self.handle, int(tx), int(ty), int(tz), int(threads)), self.handle)
+    def set_tiles(self, tx: int, ty: int, tz: int = 1, threads: int = 256, ctas_per_sm: int = 0) -> None:
+        _bcheck(self._lib.mph_batch_set_tiles(self.handle, int(tx), int(ty), int(tz), int(threads), int(ctas_per_sm)),
+                self.handle)
 
     def autotune(self, steps: int = 32) -> list[dict]:
         cap = 64
         trials = (N.BatchTrial * cap)()
         cnt = C.c_int(0)
         _bcheck(self._lib.mph_batch_autotune(self.handle, int(steps), trials, cap, C.byref(cnt)), self.handle)
-        return [{"tile": tuple(trials[k].tile), "threads": trials[k].threads, "ms_per_step": trials[k].ms_per_step}
+        return [{"tile": tuple(trials[k].tile), "threads": trials[k].threads, "ctas_per_sm": trials[k].ctas_per_sm,
+                 "capacity": trials[k].capacity, "ms_per_step": trials[k].ms_per_step}
                 for k in range(min(cnt.value, cap))]
 
     def info(self) -> dict:

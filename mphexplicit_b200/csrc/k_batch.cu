@@ -637,7 +637,7 @@ struct BatchProfile {
 
 struct mph_batch {
     int dim = 2, S = 0, n = 0, n_fluid = 0, cells = 0;
-    int tile[3] = {8, 8, 1}, threads = 256;
+    int tile[3] = {8, 8, 1}, threads = 256, occ = 2;
     int cap = 0, hmax = 0, ncol = 0, n_items = 0, grid_a = 0, grid_b = 0, sms = 0;
     size_t smem_a = 0, smem_b = 0;
     bool has_st = false;
@@ -774,7 +774,7 @@ static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& 
 
 // Tiles, items (largest first by the particle count at creation), staging
 // capacity, shared memory and persistent grid sizes for tile t and CTA size.
-static int configure(mph_batch* b, const int t[3], int threads) {
+static int configure(mph_batch* b, const int t[3], int threads, int ctas_per_sm = 2) {
     const int dim = b->dim;
     if (threads < 64 || threads > mph::kMaxThreads || threads % 32 != 0)
         return bfail(b, MPH_ERR_ARG, "threads must be a multiple of 32 in [64, 256]");
@@ -833,7 +833,9 @@ static int configure(mph_batch* b, const int t[3], int threads) {
     cudaGetDevice(&dev);
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t budget = std::min<size_t>((size_t)smem_optin, 110 * 1024) - sizeof(BScene) - 2048;
+    // shared memory for ctas_per_sm resident CTAs (228 KB per SM, 1 KB reserved per CTA)
+    const int occ = std::max(1, std::min(ctas_per_sm, 8));
+    const size_t budget = std::min<size_t>((size_t)smem_optin, (size_t)228 * 1024 / occ - 1024) - sizeof(BScene) - 2048;
     int cap = (int)std::min<long long>(max_halo + max_halo / 8 + 32, 1 << 20);
     while (cap > 64 && std::max(mph::sweep_smem(dim, 0, b->has_st, cap, hmax, ncol),
                                 mph::sweep_smem(dim, 1, b->has_st, cap, hmax, ncol)) > budget)
@@ -850,6 +852,7 @@ static int configure(mph_batch* b, const int t[3], int threads) {
     for (int d = 0; d < 3; ++d) b->tile[d] = t[d];
     if (dim == 2) b->tile[2] = 1;
     b->threads = threads;
+    b->occ = occ;
     b->cap = cap;
     b->hmax = hmax;
     b->ncol = ncol;
@@ -1184,11 +1187,12 @@ extern "C" int mph_batch_get_state(mph_batch* b, double* xyz, double* vel) {
     return MPH_OK;
 }
 
-extern "C" int mph_batch_set_tiles(mph_batch* b, int tx, int ty, int tz, int threads) {
+extern "C" int mph_batch_set_tiles(mph_batch* b, int tx, int ty, int tz, int threads, int ctas_per_sm) {
     if (!b) return bfail(nullptr, MPH_ERR_ARG, "batch is NULL");
+    if (ctas_per_sm < 0 || ctas_per_sm > 8) return bfail(b, MPH_ERR_ARG, "ctas_per_sm must be in [0, 8]");
     BTRY(b, cudaStreamSynchronize(b->stream));
     const int t[3] = {tx, ty, b->dim == 3 ? tz : 1};
-    return configure(b, t, threads);
+    return configure(b, t, threads, ctas_per_sm > 0 ? ctas_per_sm : b->occ);
 }
 
 extern "C" int mph_batch_get_info(mph_batch* b, mph_batch_info* info) {
@@ -1202,6 +1206,7 @@ extern "C" int mph_batch_get_info(mph_batch* b, mph_batch_info* info) {
     info->fluid_particles = b->n_fluid;
     for (int d = 0; d < 3; ++d) info->tile[d] = b->tile[d];
     info->threads = b->threads;
+    info->ctas_per_sm = b->occ;
     info->items = b->n_items;
     info->capacity = b->cap;
     info->grid_a = b->grid_a;
@@ -1241,20 +1246,22 @@ extern "C" int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* tria
     if (!b || steps < 1) return bfail(b, MPH_ERR_ARG, "bad arguments");
     int rc = check_ctl(b);
     if (rc != MPH_OK) return rc;
-    std::vector<std::array<int, 4>> cand;
+    std::vector<std::array<int, 5>> cand;  // tile x, y, z, CTA size, CTAs per SM the staging is sized for
     if (b->dim == 2) {
         const int ts[][2] = {{4, 4}, {4, 8}, {8, 4}, {8, 8}, {8, 16}, {16, 8}, {12, 12}, {16, 16}};
         for (auto& t : ts)
-            for (int th : {128, 256}) cand.push_back({t[0], t[1], 1, th});
+            for (int th : {128, 256})
+                for (int oc : {2, 3, 4}) cand.push_back({t[0], t[1], 1, th, oc});
     } else {
         const int ts[][3] = {{1, 2, 2}, {2, 2, 2}, {2, 2, 4}, {2, 4, 4}, {4, 4, 4}, {1, 1, 4}, {1, 2, 4}};
         for (auto& t : ts)
-            for (int th : {128, 256}) cand.push_back({t[0], t[1], t[2], th});
+            for (int th : {128, 256})
+                for (int oc : {1, 2}) cand.push_back({t[0], t[1], t[2], th, oc});
     }
     const bool prof = b->prof.on;
     b->prof.on = false;
     const long long steps0 = b->steps, launches0 = b->launches;
-    const int keep[3] = {b->tile[0], b->tile[1], b->tile[2]}, keep_threads = b->threads;
+    const int keep[3] = {b->tile[0], b->tile[1], b->tile[2]}, keep_threads = b->threads, keep_occ = b->occ;
     BatchBackup k;
     const size_t n = (size_t)b->n;
     cudaError_t e = cudaSuccess;
@@ -1283,7 +1290,7 @@ extern "C" int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* tria
     const int rounds = std::max(1, (steps + mph::kGraphSteps - 1) / mph::kGraphSteps);
     for (size_t ci = 0; ci < cand.size() && rc == MPH_OK; ++ci) {
         const int t[3] = {cand[ci][0], cand[ci][1], cand[ci][2]};
-        rc = configure(b, t, cand[ci][3]);
+        rc = configure(b, t, cand[ci][3], cand[ci][4]);
         if (rc != MPH_OK) {  // a shape this GPU cannot hold: skip it
             cudaGetLastError();
             rc = MPH_OK;
@@ -1305,6 +1312,8 @@ extern "C" int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* tria
             trials[nt].tile[1] = b->tile[1];
             trials[nt].tile[2] = b->tile[2];
             trials[nt].threads = b->threads;
+            trials[nt].ctas_per_sm = b->occ;
+            trials[nt].capacity = b->cap;
             trials[nt].ms_per_step = per;
         }
         ++nt;
@@ -1319,9 +1328,9 @@ extern "C" int mph_batch_autotune(mph_batch* b, int steps, mph_batch_trial* tria
     if (rc == MPH_OK) {
         if (best_i >= 0) {
             const int t[3] = {cand[best_i][0], cand[best_i][1], cand[best_i][2]};
-            rc = configure(b, t, cand[best_i][3]);
+            rc = configure(b, t, cand[best_i][3], cand[best_i][4]);
         } else {
-            rc = configure(b, keep, keep_threads);
+            rc = configure(b, keep, keep_threads, keep_occ);
         }
     }
     if (rc == MPH_OK) {

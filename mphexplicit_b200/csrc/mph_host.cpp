@@ -929,7 +929,8 @@ static int d2h(mph_ctx* ctx, T* dst, const T* src, size_t count) {
 extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, double* xyz, double* vel, double* force,
                              int* neighbor_count, double* density_a, double* vol_strain_p, double* virial_pressure) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    TRY(sync_state(ctx));
+    // the mixed forms compute these output-only arrays on demand
+    if (force || neighbor_count || density_a) TRY(sync_state(ctx));
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     TRY(d2h(ctx, particle_index, d.pidx[d.cur], n));
@@ -947,7 +948,6 @@ extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, doubl
 
 extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    TRY(sync_state(ctx));
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     cudaStream_t st = ctx->stream;

@@ -153,6 +153,7 @@ def test_batch_autotune_keeps_state_and_picks_a_timed_shape():
     info = b.info()
     best = min(trials, key=lambda t: t["ms_per_step"])
     assert tuple(info["tile"][:2]) == tuple(best["tile"][:2]) and info["threads"] == best["threads"]
+    assert info["ctas_per_sm"] == best["ctas_per_sm"] and info["capacity"] == best["capacity"]
     assert info["steps"] == 20
     b.step(30)
     xa, va = b.state()
@@ -160,7 +161,7 @@ def test_batch_autotune_keeps_state_and_picks_a_timed_shape():
     # the same steps without the autotuner: default shape, then the chosen one
     c = M.Batch(scs)
     c.step(20)
-    c.set_tiles(best["tile"][0], best["tile"][1], best["tile"][2], best["threads"])
+    c.set_tiles(best["tile"][0], best["tile"][1], best["tile"][2], best["threads"], best["ctas_per_sm"])
     c.step(30)
     xb, vb = c.state()
     c.close()
