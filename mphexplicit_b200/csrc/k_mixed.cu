@@ -183,8 +183,8 @@ __global__ void k_mix_rank(int n, const int* __restrict__ keys, const int* __res
 
 // Home cell and FP32 positions after a sort (sorted order).
 __global__ void k_mix_home(SimConst c, MixConst m, const double4* __restrict__ pos, const int* __restrict__ keys,
-                           const double4* __restrict__ vel, int* __restrict__ home, float4* __restrict__ p32,
-                           float4* __restrict__ p32lo, float4* __restrict__ v32) {
+                           const double4* __restrict__ vel, int* __restrict__ home, float4* __restrict__ phl,
+                           float4* __restrict__ p32, float4* __restrict__ v32) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     int k = keys[i];
@@ -193,8 +193,9 @@ __global__ void k_mix_home(SimConst c, MixConst m, const double4* __restrict__ p
     home[i] = h;
     float4 hi, lo;
     rel32(c, m, pos[i], h, hi, lo);
+    phl[2 * (size_t)i] = hi;
+    phl[2 * (size_t)i + 1] = lo;
     p32[i] = hi;
-    p32lo[i] = lo;
     const double4 v = vel[i];
     v32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.0f);
 }
@@ -286,7 +287,7 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
 __global__ void __launch_bounds__(256)
 k_mix_move(SimConst c, MixConst m, const int* __restrict__ cellstart, double4* __restrict__ pos,
            double4* __restrict__ vel, const double4* __restrict__ snap, const double* __restrict__ wall_center,
-           const int* __restrict__ home, float4* __restrict__ p32, float4* __restrict__ p32lo,
+           const int* __restrict__ home, float4* __restrict__ phl, float4* __restrict__ p32,
            float4* __restrict__ v32, StepScalars* __restrict__ scal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double s2 = 0.0;
@@ -322,8 +323,9 @@ k_mix_move(SimConst c, MixConst m, const int* __restrict__ cellstart, double4* _
         pos[i] = p;
         float4 hi, lo;
         rel32(c, m, p, home[i], hi, lo);
+        phl[2 * (size_t)i] = hi;
+        phl[2 * (size_t)i + 1] = lo;
         p32[i] = hi;
-        p32lo[i] = lo;
         v32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.0f);
         const double4 q = snap[i];
         const double d0 = omod_fast(p.x - q.x + c.half_width[0], c.width[0]) - c.half_width[0];
@@ -363,30 +365,25 @@ __device__ __forceinline__ void load_tables(const MixConst& m, SharedTables& t) 
     __syncthreads();
 }
 
-// FP64 minimum-image displacement and 1/r from an FP32 seed plus one Newton
-// step (relative error ~1e-14), for the FP64 pressure core.
-__device__ __forceinline__ void disp64(const SimConst& c, const double4& pi, const double4& pj, double& dx, double& dy,
-                                       double& dz) {
-    dx = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-    dy = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-    dz = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
-}
+// 1/sqrt from an FP32 seed plus one Newton step (relative error ~1e-14), for
+// the FP64 density pairs.
 __device__ __forceinline__ double rsqrt64(double r2) {
     const double y = (double)rsqrtf((float)r2);
     return y * (1.5 - 0.5 * r2 * y * y);
 }
 
 // Sweep A: DensityP and DivergenceP over the short part of the list with the
-// exact FP32 displacement (S64: in FP64 from the FP64 positions), plus, with
+// exact FP32 displacement (S64: pair arithmetic in FP64, the displacement
+// assembled in FP64 from the hi/lo parts, FP32 velocities), plus, with
 // surface tension, DensityA and GravityCenter over all of it; epilogue:
 // coefficients, PressureP, PressureA (main.cpp:1631-1662, 1735-1740, 1831-1906).
 template <bool ST, bool RATIO, bool S64>
 __global__ void __launch_bounds__(128)
-k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p32lo, const float4* __restrict__ v32,
+k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v32,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
         float4* __restrict__ pv, float4* __restrict__ gca, double* __restrict__ strain_out,
         double* __restrict__ div_out, double* __restrict__ dens_a_out, double* __restrict__ wall_center,
-        const SimConst c, const double4* __restrict__ pos64, const double4* __restrict__ vel64,
+        const SimConst c, const double4* __restrict__ vel64,
         double4* __restrict__ press64) {
     __shared__ SharedTables tb;
     load_tables(m, tb);
@@ -396,14 +393,9 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
         if (t >= 2) wall_center[3 * t + d] += c.wall_velocity[t][d] * c.dt;
     }
     if (i >= m.n) return;
-    const float4 pi = p32[i];
-    const float4 li = p32lo[i];
+    const float4 pi = phl[2 * (size_t)i];
+    const float4 li = phl[2 * (size_t)i + 1];
     const float4 vi = v32[i];
-    double4 pid = make_double4(0, 0, 0, 0), vid = make_double4(0, 0, 0, 0);
-    if (S64) {
-        pid = pos64[i];
-        vid = vel64[i];
-    }
     const int ti = __float_as_int(pi.w);
     const int ns = cnt_short[i];
     const int na = ST ? cnt_all[i] : ns;
@@ -414,27 +406,30 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
     const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
     for_entries(tab, n, ns, [&](unsigned e) {
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
-        const float4 pj = p32[j];
-        const float4 dh = tb.dhi[code];
+        float4 pj, lj;
+        ldg_pv(phl, j, pj, lj);  // {hi, lo} in one 256-bit load
+        const float4 dh = tb.dhi[code], dl = tb.dlo[code];
         float dx, dy, dz;
         if (S64) {
-            double dxd, dyd, dzd;
-            disp64(c, pid, pos64[j], dxd, dyd, dzd);
+            // FP64 displacement: the hi difference plus the cell offset is exact in
+            // FP32 (grid multiples), the lo parts carry the rest to ~1e-14 l0
+            const double dxd = (double)((pj.x - pi.x) + dh.x) + (((double)lj.x - (double)li.x) + (double)dl.x);
+            const double dyd = (double)((pj.y - pi.y) + dh.y) + (((double)lj.y - (double)li.y) + (double)dl.y);
+            const double dzd = (double)((pj.z - pi.z) + dh.z) + (((double)lj.z - (double)li.z) + (double)dl.z);
             const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
             if (r2d <= c.rp2) {
                 const double y = rsqrt64(r2d);
                 const double q = 1.0 - r2d * y * m.inv_rp_d;
                 spd += m.cp_d * q * q;
                 const double dw = m.cp_m2_d * q;
-                const double4 vj = vel64[j];
-                sdd -= ((vj.x - vid.x) * dxd + (vj.y - vid.y) * dyd + (vj.z - vid.z) * dzd) * y * dw;
+                const float4 vj = v32[j];
+                sdd -= (((double)vj.x - (double)vi.x) * dxd + ((double)vj.y - (double)vi.y) * dyd +
+                        ((double)vj.z - (double)vi.z) * dzd) * y * dw;
             }
             dx = (float)dxd;
             dy = (float)dyd;
             dz = (float)dzd;
         } else {
-            const float4 lj = p32lo[j];
-            const float4 dl = tb.dlo[code];
             dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
             dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
             dz = ((pj.z - pi.z) + dh.z) + ((lj.z - li.z) + dl.z);
@@ -455,7 +450,7 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
     if (ST) {  // surface tension only: the long part
         for_entries(tab + (size_t)(m.cap_s >> 2) * n, n, na - ns, [&](unsigned e) {
             const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
-            const float4 pj = p32[j];
+            const float4 pj = phl[2 * (size_t)j];
             const float4 dh = tb.dhi[code];
             const float dx = (pj.x - pi.x) + dh.x, dy = (pj.y - pi.y) + dh.y, dz = (pj.z - pi.z) + dh.z;
             const float r2 = dx * dx + dy * dy + dz * dz;
@@ -485,7 +480,10 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
     }
     pv[2 * (size_t)i] = pi;
     pv[2 * (size_t)i + 1] = make_float4(vi.x, vi.y, vi.z, (float)pp);
-    if (S64) press64[i] = make_double4(vid.x, vid.y, vid.z, pp);
+    if (S64) {
+        const double4 vid = vel64[i];
+        press64[i] = make_double4(vid.x, vid.y, vid.z, pp);
+    }
     strain_out[i] = strain;
     div_out[i] = div;
 }
@@ -499,8 +497,8 @@ k_mix_a(MixConst m, const float4* __restrict__ p32, const float4* __restrict__ p
 // (main.cpp:1908-2010).
 template <bool ST, bool RATIO, bool WALLS>
 __global__ void __launch_bounds__(128, MPH_MIXB_MINB_FUSED)
-k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ p32,
-        const float4* __restrict__ p32lo, const float4* __restrict__ pv, const float4* __restrict__ gca,
+k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ phl,
+        const float4* __restrict__ pv, const float4* __restrict__ gca,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
         const double4* __restrict__ vel, double4* __restrict__ vel_out, double4* __restrict__ force,
         StepScalars* __restrict__ scal) {
@@ -513,8 +511,8 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         if (!WALLS) vel_out[i] = vel[i];
         return;
     }
-    const float4 pi = p32[i];
-    const float4 li = p32lo[i];
+    const float4 pi = phl[2 * (size_t)i];
+    const float4 li = phl[2 * (size_t)i + 1];
     const float4 vi = pv[2 * (size_t)i + 1];
     const int ti = __float_as_int(pi.w);
     float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -530,7 +528,7 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
         const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
         float4 pj, vj;
         ldg_pv(pv, j, pj, vj);
-        const float4 lj = p32lo[j];
+        const float4 lj = phl[2 * (size_t)j + 1];
         const float4 dh = tb.dhi[code], dl = tb.dlo[code];
         const float dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
         const float dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
@@ -669,10 +667,10 @@ struct MixedState {
     int* counts = nullptr;
     int* tmp = nullptr;
     int* home = nullptr;
-    float4* p32 = nullptr;
-    float4* p32lo = nullptr;
+    float4* phl = nullptr;  // [2n]: {hi position + type, lo position} per particle (home-cell relative)
+    float4* p32 = nullptr;  // [n]: the hi parts alone, for the table build
     float4* v32 = nullptr;
-    float4* pv = nullptr;  // [2n]: {p32, (v, PressureP)} per particle, written by sweep A
+    float4* pv = nullptr;  // [2n]: {hi position + type, (v, PressureP)} per particle, written by sweep A
     float4* gca = nullptr;
     unsigned* list = nullptr;
     int cap = 0;          // cap_s + cap_l rows
@@ -687,7 +685,7 @@ struct MixedState {
 };
 
 static void mfree(MixedState* m) {
-    void* ptrs[] = {m->keys_unsorted, m->slot, m->counts, m->tmp, m->home, m->p32, m->p32lo, m->v32, m->pv,
+    void* ptrs[] = {m->keys_unsorted, m->slot, m->counts, m->tmp, m->home, m->phl, m->p32, m->v32, m->pv,
                     m->gca, m->list, m->cnt_short, m->cnt_all};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -734,8 +732,8 @@ int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, 
                    d.snap, s);
     d.cur = b;
     d.vcur = vb;
-    k_mix_home<<<blocks(n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->p32,
-                                              m->p32lo, m->v32);
+    k_mix_home<<<blocks(n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->phl,
+                                              m->p32, m->v32);
     nl += 6;
     for (int attempt = 0; attempt < 3; ++attempt) {
         MTRY(cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), s));
@@ -767,9 +765,9 @@ void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wa
     const int nb = blocks(c.n, 128);
     double* wc = advance_wall ? d.wall_center : nullptr;
 #define MIX_A(ST, RATIO, S64)                                                                                   \
-    k_mix_a<ST, RATIO, S64><<<nb, 128, 0, s>>>(m->mc, m->p32, m->p32lo, m->v32, m->list, m->cnt_short,          \
+    k_mix_a<ST, RATIO, S64><<<nb, 128, 0, s>>>(m->mc, m->phl, m->v32, m->list, m->cnt_short,          \
                                                m->cnt_all, m->pv, m->gca, d.strain_p, d.div_p, d.dens_a, wc, c, \
-                                               d.pos[d.cur], d.vel[d.vcur], d.press)
+                                               d.vel[d.vcur], d.press)
 #define MIX_A2(ST, RATIO) \
     if (m->s64) MIX_A(ST, RATIO, true); else MIX_A(ST, RATIO, false)
     if (m->mc.has_st) {
@@ -787,7 +785,7 @@ static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t 
     const int nb = blocks(c.n, 128);
     double4* vout = WALLS ? nullptr : d.vel[1 - d.vcur];
 #define MIX_B1(ST, RATIO)                                                                                   \
-    k_mix_b<ST, RATIO, WALLS><<<nb, 128, 0, s>>>(m->mc, c, d.cellstart, m->p32, m->p32lo, m->pv, m->gca,   \
+    k_mix_b<ST, RATIO, WALLS><<<nb, 128, 0, s>>>(m->mc, c, d.cellstart, m->phl, m->pv, m->gca,   \
                                                  m->list, m->cnt_short, m->cnt_all, d.vel[d.vcur], vout,   \
                                                  d.force, d.scal)
     if (m->mc.has_st) {
@@ -806,7 +804,7 @@ int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) 
 
 void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     k_mix_move<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap,
-                                                d.wall_center, m->home, m->p32, m->p32lo, m->v32, d.scal);
+                                                d.wall_center, m->home, m->phl, m->p32, m->v32, d.scal);
     m->exported = false;
 }
 
@@ -907,8 +905,8 @@ int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, De
     if (e == cudaSuccess) e = malloc_n(&m->counts, 2 * (size_t)c.tot + 1);
     if (e == cudaSuccess) e = malloc_n(&m->tmp, n);
     if (e == cudaSuccess) e = malloc_n(&m->home, n);
+    if (e == cudaSuccess) e = malloc_n(&m->phl, 2 * n);
     if (e == cudaSuccess) e = malloc_n(&m->p32, n);
-    if (e == cudaSuccess) e = malloc_n(&m->p32lo, n);
     if (e == cudaSuccess) e = malloc_n(&m->v32, n);
     if (e == cudaSuccess) e = malloc_n(&m->pv, 2 * n);
     if (e == cudaSuccess) e = malloc_n(&m->gca, n);
@@ -972,8 +970,8 @@ int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, s
 
 int mixed_import(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err) {
     // positions/velocities changed from the host: refresh the FP32 copies
-    k_mix_home<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->p32,
-                                                m->p32lo, m->v32);
+    k_mix_home<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.pos[d.cur], d.keys, d.vel[d.vcur], m->home, m->phl,
+                                                m->p32, m->v32);
     MTRY(cudaGetLastError());
     m->exported = false;
     return MPH_OK;
