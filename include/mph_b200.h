@@ -227,6 +227,27 @@ int mph_write_vtk_arrays(const char* path, int n, const int* type, const double*
  * out[4]=kinetic energy. */
 int mph_conserved_sums(mph_ctx* ctx, double out[5]);
 
+/* ---- exact checkpoint (no reference counterpart: the reference restarts from
+ * a *.prof file, readGridFile main.cpp:541-640 with iStep = Time/Dt at :371,
+ * whose "%e" text keeps ~7 digits and drops the moving walls' centres) -----
+ * The file holds Time (in the grid header), the step count, the parameters
+ * with Wall2/3 Center set to the centres reached, and every particle's type,
+ * ParticleIndex, position and velocity in FP64, in the context's current
+ * (cell-sorted) order -- the order of the *.prof file the reference would
+ * write at that time.  Creating a context from it (mph_create with the
+ * returned arrays) is the reference's restart from that *.prof, exactly. */
+int mph_write_checkpoint(mph_ctx* ctx, const char* path);
+/* The same file from host arrays (no GPU). */
+int mph_write_checkpoint_arrays(const char* path, const mph_params* p, const mph_grid_header* h, int dim,
+                                long long step, const int* type, const int* particle_index,
+                                const double* xyz, const double* vel);
+/* Parameters, grid header (Time, particle count, domain), dimension and step. */
+int mph_read_checkpoint_header(const char* path, mph_params* p, mph_grid_header* h, int* dim, long long* step);
+/* Everything, particles into caller arrays of `capacity` particles;
+ * MPH_ERR_IO for a missing, foreign or truncated file. */
+int mph_read_checkpoint(const char* path, mph_params* p, mph_grid_header* h, int* dim, long long* step,
+                        int capacity, int* type, int* particle_index, double* xyz, double* vel);
+
 /* ---- measurement hooks (no reference counterpart: the reference only has
  * clock() totals, main.cpp:287-288, 456-465) ---------------------------- */
 

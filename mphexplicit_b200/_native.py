@@ -181,6 +181,13 @@ SIGNATURES = {
     "mph_write_prof": (_I, [_P, C.c_char_p]),
     "mph_write_vtk_arrays": (_I, [C.c_char_p, _I, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp]),
     "mph_conserved_sums": (_I, [_P, _dp]),
+    "mph_write_checkpoint": (_I, [_P, C.c_char_p]),
+    "mph_write_checkpoint_arrays": (_I, [C.c_char_p, C.POINTER(Params), C.POINTER(GridHeader), _I, C.c_longlong,
+                                         _ip, _ip, _dp, _dp]),
+    "mph_read_checkpoint_header": (_I, [C.c_char_p, C.POINTER(Params), C.POINTER(GridHeader), _ip,
+                                        C.POINTER(C.c_longlong)]),
+    "mph_read_checkpoint": (_I, [C.c_char_p, C.POINTER(Params), C.POINTER(GridHeader), _ip, C.POINTER(C.c_longlong),
+                                 _I, _ip, _ip, _dp, _dp]),
     "mph_stream": (_P, [_P]),
     "mph_launch_count": (C.c_longlong, [_P]),
     "mph_profile_enable": (_I, [_P, _I]),

@@ -33,6 +33,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <nvtx3/nvToolsExt.h>
 #include "mph_internal.h"
 #include "mph_pair32.cuh"
 
@@ -881,12 +882,14 @@ static int configure(mph_batch* b, const int t[3], int threads, int ctas_per_sm 
     return MPH_OK;
 }
 
-// Profiling: CUDA events around launch groups when enabled (direct launches).
+// Launch groups: an NVTX range each, and CUDA events around them when
+// profiling is enabled (direct launches).
 struct BLaunch {
     mph_batch* b;
     int id = -1, count;
     cudaEvent_t a = nullptr;
     BLaunch(mph_batch* bb, const char* name, int c) : b(bb), count(c) {
+        nvtxRangePushA(name);
         BatchProfile& p = b->prof;
         if (!p.on) return;
         for (size_t k = 0; k < p.names.size(); ++k)
@@ -901,6 +904,7 @@ struct BLaunch {
         cudaEventRecord(a, b->stream);
     }
     ~BLaunch() {
+        nvtxRangePop();
         b->launches += count;
         if (id < 0) return;
         cudaEvent_t e = nullptr;

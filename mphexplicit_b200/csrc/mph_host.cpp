@@ -17,6 +17,7 @@
 #include <vector>
 #include <algorithm>
 
+#include <nvtx3/nvToolsExt.h>
 #include "mph_internal.h"
 #include "mph_io.h"
 #include "mph_mixed.h"
@@ -98,7 +99,8 @@ static cudaEvent_t take_event(mph_ctx* ctx) {
     return e;
 }
 
-// Brackets one launch (or one group of launches) of a named kernel: counts it
+// Brackets one launch (or one group of launches) of a named kernel: counts it,
+// marks it as an NVTX range (visible to Nsight Systems on the host timeline)
 // and, when profiling is on, records CUDA events around it on the ctx stream.
 struct Launch {
     mph_ctx* ctx;
@@ -106,6 +108,7 @@ struct Launch {
     int count = 1;
     cudaEvent_t a = nullptr;
     Launch(mph_ctx* c, const char* name) : ctx(c) {
+        nvtxRangePushA(name);
         Profiler& p = ctx->prof;
         if (!p.on) return;
         for (size_t k = 0; k < p.names.size(); ++k)
@@ -120,6 +123,7 @@ struct Launch {
         cudaEventRecord(a, ctx->stream);
     }
     ~Launch() {
+        nvtxRangePop();
         ctx->launches += count;
         if (id < 0) return;
         cudaEvent_t b = take_event(ctx);
@@ -1076,6 +1080,26 @@ extern "C" int mph_write_prof(mph_ctx* ctx, const char* path) {
     mph_grid_header h = ctx->h;
     h.time = ctx->time;
     const int st = mph_write_grid_file(path, &h, type.data(), x.data(), v.data());
+    if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
+    return MPH_OK;
+}
+
+extern "C" int mph_write_checkpoint(mph_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    const size_t n = (size_t)ctx->n;
+    std::vector<int> type(n), pidx(n);
+    std::vector<double> x(3 * n), v(3 * n);
+    TRY(mph_get_state(ctx, pidx.data(), type.data(), x.data(), v.data(), nullptr, nullptr, nullptr, nullptr, nullptr));
+    double wc[12];
+    CUDA_TRY(ctx, cudaMemcpyAsync(wc, ctx->d.wall_center, sizeof(wc), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    mph_params p = ctx->p;
+    for (int t = 2; t < MPH_TYPE_COUNT; ++t)  // the wall centres reached (calculateWall, main.cpp:2013-2053)
+        for (int k = 0; k < 3; ++k) p.wall_center[t][k] = wc[3 * t + k];
+    mph_grid_header h = ctx->h;
+    h.time = ctx->time;
+    const int st = mph_write_checkpoint_arrays(path, &p, &h, ctx->dim, ctx->step, type.data(), pidx.data(), x.data(),
+                                               v.data());
     if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
     return MPH_OK;
 }

@@ -3,7 +3,8 @@
 //   *.grid  : readGridFile     (main.cpp:541-640), writeProfFile (672-696)
 //   *.vtk   : writeVtkFile     (main.cpp:698-834)
 // The sscanf/fprintf patterns are the reference's, so files round-trip
-// byte-for-byte between the two programs.
+// byte-for-byte between the two programs.  Also the exact binary checkpoint
+// (no reference counterpart; see mph_write_checkpoint_arrays).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -133,6 +134,87 @@ extern "C" int mph_write_grid_file(const char* path, const mph_grid_header* h, c
     const int bad = std::ferror(fp);
     std::fclose(fp);
     return bad ? MPH_ERR_IO : MPH_OK;
+}
+
+// ---- exact binary checkpoint ---------------------------------------------------
+// Layout (native byte order, the struct layouts of mph_b200.h):
+//   char magic[8] = "MPHCKPT1"; int32 dim; int32 n; int64 step;
+//   mph_params; mph_grid_header; int32 type[n]; int32 particle_index[n];
+//   double xyz[3n]; double vel[3n]
+namespace {
+const char kCkptMagic[8] = {'M', 'P', 'H', 'C', 'K', 'P', 'T', '1'};
+
+struct CkptHead {
+    char magic[8];
+    int dim, n;
+    long long step;
+};
+
+int read_ckpt_head(FILE* fp, CkptHead* hd, mph_params* p, mph_grid_header* h) {
+    if (std::fread(hd, sizeof(*hd), 1, fp) != 1 || std::memcmp(hd->magic, kCkptMagic, 8) != 0) return MPH_ERR_IO;
+    if (std::fread(p, sizeof(*p), 1, fp) != 1 || std::fread(h, sizeof(*h), 1, fp) != 1) return MPH_ERR_IO;
+    if ((hd->dim != 2 && hd->dim != 3) || hd->n < 0 || hd->n != h->particle_count) return MPH_ERR_IO;
+    return MPH_OK;
+}
+}  // namespace
+
+extern "C" int mph_write_checkpoint_arrays(const char* path, const mph_params* p, const mph_grid_header* h, int dim,
+                                           long long step, const int* type, const int* particle_index,
+                                           const double* xyz, const double* vel) {
+    if (!path || !p || !h || (dim != 2 && dim != 3) || h->particle_count < 0 ||
+        (h->particle_count > 0 && (!type || !particle_index || !xyz || !vel)))
+        return MPH_ERR_ARG;
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return MPH_ERR_IO;
+    CkptHead hd{};
+    std::memcpy(hd.magic, kCkptMagic, 8);
+    hd.dim = dim;
+    hd.n = h->particle_count;
+    hd.step = step;
+    const size_t n = (size_t)h->particle_count;
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, fp) == 1 && std::fwrite(p, sizeof(*p), 1, fp) == 1 &&
+              std::fwrite(h, sizeof(*h), 1, fp) == 1;
+    if (ok && n > 0)
+        ok = std::fwrite(type, sizeof(int), n, fp) == n && std::fwrite(particle_index, sizeof(int), n, fp) == n &&
+             std::fwrite(xyz, sizeof(double), 3 * n, fp) == 3 * n &&
+             std::fwrite(vel, sizeof(double), 3 * n, fp) == 3 * n;
+    ok = std::fflush(fp) == 0 && ok;
+    std::fclose(fp);
+    return ok ? MPH_OK : MPH_ERR_IO;
+}
+
+extern "C" int mph_read_checkpoint_header(const char* path, mph_params* p, mph_grid_header* h, int* dim,
+                                          long long* step) {
+    if (!path || !p || !h) return MPH_ERR_ARG;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return MPH_ERR_IO;
+    CkptHead hd{};
+    const int st = read_ckpt_head(fp, &hd, p, h);
+    std::fclose(fp);
+    if (st != MPH_OK) return st;
+    if (dim) *dim = hd.dim;
+    if (step) *step = hd.step;
+    return MPH_OK;
+}
+
+extern "C" int mph_read_checkpoint(const char* path, mph_params* p, mph_grid_header* h, int* dim, long long* step,
+                                   int capacity, int* type, int* particle_index, double* xyz, double* vel) {
+    if (!path || !p || !h || !type || !particle_index || !xyz || !vel) return MPH_ERR_ARG;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) return MPH_ERR_IO;
+    CkptHead hd{};
+    int st = read_ckpt_head(fp, &hd, p, h);
+    if (st == MPH_OK && hd.n > capacity) st = MPH_ERR_ARG;
+    const size_t n = (size_t)hd.n;
+    if (st == MPH_OK && n > 0 &&
+        (std::fread(type, sizeof(int), n, fp) != n || std::fread(particle_index, sizeof(int), n, fp) != n ||
+         std::fread(xyz, sizeof(double), 3 * n, fp) != 3 * n || std::fread(vel, sizeof(double), 3 * n, fp) != 3 * n))
+        st = MPH_ERR_IO;  // truncated
+    std::fclose(fp);
+    if (st != MPH_OK) return st;
+    if (dim) *dim = hd.dim;
+    if (step) *step = hd.step;
+    return MPH_OK;
 }
 
 namespace mph {

@@ -115,6 +115,42 @@ def write_vtk_arrays(path: str, state: dict) -> None:
                                          _dp(f64["vol_strain_p"]), _dp(f64["virial_pressure"])))
 
 
+@dataclass
+class Checkpoint:
+    """Contents of an exact checkpoint (mph_write_checkpoint): the particles in
+    the order of the *.prof file the reference would write at that time."""
+    params: N.Params
+    header: N.GridHeader
+    dim: int
+    step: int
+    type: np.ndarray
+    particle_index: np.ndarray
+    xyz: np.ndarray
+    vel: np.ndarray
+
+
+def write_checkpoint_arrays(path: str, ck: Checkpoint) -> None:
+    t = np.ascontiguousarray(ck.type, np.int32)
+    pi = np.ascontiguousarray(ck.particle_index, np.int32)
+    x = np.ascontiguousarray(ck.xyz, np.float64)
+    v = np.ascontiguousarray(ck.vel, np.float64)
+    _check(N.load().mph_write_checkpoint_arrays(path.encode(), C.byref(ck.params), C.byref(ck.header), int(ck.dim),
+                                                int(ck.step), _ip(t), _ip(pi), _dp(x), _dp(v)))
+
+
+def read_checkpoint(path: str) -> Checkpoint:
+    lib = N.load()
+    p, h = N.Params(), N.GridHeader()
+    dim, step = C.c_int(0), C.c_longlong(0)
+    _check(lib.mph_read_checkpoint_header(path.encode(), C.byref(p), C.byref(h), C.byref(dim), C.byref(step)))
+    n = h.particle_count
+    t, pi = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    x, v = np.zeros((n, 3)), np.zeros((n, 3))
+    _check(lib.mph_read_checkpoint(path.encode(), C.byref(p), C.byref(h), C.byref(dim), C.byref(step), n, _ip(t),
+                                   _ip(pi), _dp(x), _dp(v)))
+    return Checkpoint(p, h, dim.value, step.value, t, pi, x, v)
+
+
 def compute_constants(params: N.Params, header: N.GridHeader, dim: int) -> N.Constants:
     c = N.Constants()
     _check(N.load().mph_compute_constants(C.byref(params), C.byref(header), dim, C.byref(c)))
@@ -150,6 +186,16 @@ class Solver:
     def from_files(cls, data: str, grid: str, dim: int = 3, mode: str = "fp64") -> "Solver":
         g = read_grid_file(grid)
         return cls(read_data_file(data), g.header, g.type, g.xyz, g.vel, dim=dim, mode=mode)
+
+    @classmethod
+    def from_checkpoint(cls, path: str, mode: str = "fp64") -> "Solver":
+        """Restart from an exact checkpoint (the reference's restart from the
+        *.prof file of that time, without its text rounding)."""
+        ck = read_checkpoint(path)
+        return cls(ck.params, ck.header, ck.type, ck.xyz, ck.vel, dim=ck.dim, mode=mode)
+
+    def write_checkpoint(self, path: str) -> None:
+        _check(self._lib.mph_write_checkpoint(self._ctx, path.encode()), self._ctx)
 
     # -- stepping --------------------------------------------------------
     def step(self, nsteps: int = 1) -> None:

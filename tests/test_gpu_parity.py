@@ -128,6 +128,34 @@ def test_state_round_trip_and_step_continuity():
         assert_same(a.state()[key], b.state()[key], key)
 
 
+def test_checkpoint_restart_is_the_reference_restart_exactly():
+    """A checkpoint keeps the state in the order of the *.prof file of that
+    time with the wall centres reached; restarting from it equals the
+    reference (oracle) restarted from the same state, bit for bit, and the
+    file maps every particle back to its original id."""
+    case = GoldenCase("moving_walls")
+    s = solver_for(case)
+    s.step(37)
+    before = s.state()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "run.ckpt")
+        s.write_checkpoint(path)
+        ck = M.read_checkpoint(path)
+        r = M.Solver.from_checkpoint(path)
+    assert ck.step == 37 and ck.header.time == s.info()["time"]
+    assert np.array_equal(ck.particle_index, before["particle_index"])
+    assert np.array_equal(ck.xyz, before["xyz"]) and np.array_equal(ck.vel, before["vel"])
+    assert any(ck.params.wall_center[t][k] != s.params.wall_center[t][k] for t in (2, 3) for k in range(3))
+    o = po.Oracle(ck.params, ck.header, ck.type, ck.xyz, ck.vel, ck.dim)
+    r.step(25)
+    o.step(25)
+    got, ref = r.state(), o.state()
+    for key in STATE_KEYS:
+        assert_same(got[key], ref[key], key)
+    r.close()
+    s.close()
+
+
 def test_nonfinite_state_is_reported_not_trapped():
     """A NaN velocity injected from the host is caught by the device-side
     finiteness flag and returned as MPH_ERR_NONFINITE; the context stays usable."""

@@ -216,3 +216,32 @@ def test_batch_rejects_bad_scenes_before_touching_the_gpu():
     mixed_dim = scenes.dam_break_3d(fluid=(4, 4, 4), box=(8, 6, 8))
     with pytest.raises(ValueError):
         M.Batch([good[0], mixed_dim])
+
+
+def test_checkpoint_file_round_trip_is_exact_and_rejects_bad_files():
+    rng = np.random.default_rng(5)
+    sc = scenes.dam_break_3d(fluid=(4, 4, 5), box=(8, 6, 8), seed=2)
+    sc.params.wall_center[2][:] = [0.1, 0.2, 0.3]
+    n = sc.n
+    hdr = M.make_header(n, 0.005, [-0.1] * 3, [0.2] * 3, time=0.123456789012345678)
+    ck = M.Checkpoint(sc.params, hdr, 3, 4242, sc.type, rng.permutation(n).astype(np.int32),
+                      rng.standard_normal((n, 3)), rng.standard_normal((n, 3)) * 1e-3)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "state.ckpt")
+        M.write_checkpoint_arrays(path, ck)
+        got = M.read_checkpoint(path)
+        assert got.dim == 3 and got.step == 4242 and got.header.time == hdr.time
+        assert got.header.particle_count == n
+        for k in ("type", "particle_index", "xyz", "vel"):
+            assert np.array_equal(getattr(got, k), getattr(ck, k)), k
+        assert list(got.params.wall_center[2]) == [0.1, 0.2, 0.3] and got.params.dt == sc.params.dt
+        raw = open(path, "rb").read()
+        open(path, "wb").write(raw[:-8])  # truncated
+        with pytest.raises(M.MphError) as e:
+            M.read_checkpoint(path)
+        assert e.value.code == N.MPH_ERR_IO
+        open(path, "wb").write(b"NOTACKPT" + raw[8:])  # foreign
+        with pytest.raises(M.MphError):
+            M.read_checkpoint(path)
+        with pytest.raises(M.MphError):
+            M.read_checkpoint(os.path.join(td, "missing.ckpt"))
