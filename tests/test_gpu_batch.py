@@ -14,7 +14,7 @@ import pytest
 import mphexplicit_b200 as M
 from mphexplicit_b200 import scenes
 from oracle import pyoracle as po
-from tests.common import by_original_id, rel_l2
+from tests.common import by_original_id, micro_cases, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -177,3 +177,21 @@ def test_batch_momentum_free_droplets():
         v = vel[off[k]:off[k + 1]]
         mom = np.abs(v.sum(axis=0)) * sc.params.density[0]
         assert np.all(mom < 1e-8 * np.abs(v).sum() * sc.params.density[0] + 1e-12), (k, mom)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_batch_micro_cases_against_fp64(dim):
+    """The micro-cases of one dimension as one batch: lone particles, an
+    isolated wall, pairs across every periodic face and at every radius."""
+    cases = [(sc, steps) for (name, sc), steps in micro_cases() if sc.dim == dim]
+    steps = min(st for _, st in cases)
+    scs = [sc for sc, _ in cases]
+    xyz, vel, _ = run_batch(scs, steps)
+    off = offsets_of(scs)
+    for k, sc in enumerate(scs):
+        rx, rv = fp64_state(sc, steps)
+        a, e = int(off[k]), int(off[k + 1])
+        fl = sc.type < 2
+        err = rel_l2(vel[a:e][fl], rv[fl])
+        assert err <= TOL, (sc.name, err)
+        assert rel_l2(xyz[a:e], rx) < 1e-6, sc.name

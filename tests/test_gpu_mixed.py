@@ -11,7 +11,7 @@ import pytest
 
 import mphexplicit_b200 as M
 from mphexplicit_b200 import scenes
-from tests.common import by_original_id, rel_l2
+from tests.common import by_original_id, micro_cases, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -80,3 +80,17 @@ def test_mixed_p64_full_size_dam_break_1000_steps():
     got, _, _ = run(sc, 1000, "mixed_p64")
     err = vel_error(ref, got)
     assert err <= 1e-4, err
+
+
+@pytest.mark.parametrize("mode", ["mixed", "mixed_p64"])
+@pytest.mark.parametrize("k", range(6))
+def test_mixed_micro_cases(k, mode):
+    """The micro-cases (pairs at every radius, a lone particle, an isolated
+    wall, every periodic face, a thin 2-D grid) within the form's tolerance."""
+    (name, sc), steps = list(micro_cases())[k]
+    ref, rinfo, _ = run(sc, steps, "fp64")
+    got, ginfo, _ = run(sc, steps, mode)
+    err = vel_error(ref, got)
+    assert err <= TOL[mode], f"{name} {mode}: {err:.3e}"
+    assert rel_l2(by_original_id(got, "xyz"), by_original_id(ref, "xyz")) < 1e-6
+    assert np.array_equal(by_original_id(got, "neighbor_count"), by_original_id(ref, "neighbor_count"))

@@ -17,7 +17,7 @@ import mphexplicit_b200 as M
 from mphexplicit_b200 import _native as N
 from mphexplicit_b200 import scenes
 from oracle import pyoracle as po
-from tests.common import CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same
+from tests.common import CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same, micro_cases
 
 pytestmark = pytest.mark.gpu
 
@@ -96,6 +96,26 @@ def test_fp64_matches_oracle_fresh(k):
     for key in STATE_KEYS:
         assert_same(a[key], b[key], f"{sc.name}:{key}")
     assert s.info()["rebuild_count"] == o.rebuilds
+
+
+@pytest.mark.parametrize("k", range(6))
+def test_fp64_matches_oracle_micro(k):
+    """Pairs at every kernel radius, a lone particle, a wall out of every fluid
+    particle's reach, motion and interaction across all periodic faces, a
+    thin 2-D grid: bit-exact against the oracle (pinned to the reference on
+    the same cases)."""
+    (name, sc), steps = list(micro_cases())[k]
+    o = po.Oracle.from_scene(sc)
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim)
+    o.step(steps)
+    s.step(steps)
+    o.virial()
+    s.compute_virial()
+    a, b = s.state(), o.state()
+    for key in STATE_KEYS:
+        assert_same(a[key], b[key], f"{name}:{key}")
+    assert s.info()["rebuild_count"] == o.rebuilds
+    s.close()
 
 
 @pytest.mark.parametrize("name", ["square_drop_skip", "dam_break_small"])

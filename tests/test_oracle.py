@@ -14,7 +14,7 @@ import pytest
 
 from mphexplicit_b200 import read_data_file, read_grid_file, scenes
 from oracle import pyoracle as po
-from tests.common import CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same
+from tests.common import micro_cases, CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same
 
 
 def run_oracle(case: GoldenCase):
@@ -104,3 +104,23 @@ def test_oracle_rejects_bad_geometry():
             po.Oracle(p, h, t, x, np.zeros_like(x), 3)
     else:
         po.Oracle(p, h, t, x, np.zeros_like(x), 3).close()
+
+
+@pytest.mark.skipif(not (po.ref_available(2) and po.ref_available(3)), reason="reference build absent")
+@pytest.mark.parametrize("k", range(6))
+def test_oracle_matches_reference_micro(k):
+    """Micro-cases (pairs at every radius, a lone particle, an isolated wall,
+    every periodic face, a thin 2-D grid) against the reference itself."""
+    (name, sc), steps = list(micro_cases())[k]
+    with tempfile.TemporaryDirectory() as td:
+        d, g = os.path.join(td, "a.data"), os.path.join(td, "a.grid")
+        sc.write(d, g)
+        ref = po.run_reference(d, g, sc.dim, steps, virial=True)
+        gr = read_grid_file(g)
+        o = po.Oracle(read_data_file(d), gr.header, gr.type, gr.xyz, gr.vel, sc.dim)
+        o.step(steps)
+        o.virial()
+        s = o.state()
+        for key in STATE_KEYS:
+            assert_same(s[key], ref[key], f"{name}:{key}")
+        assert o.rebuilds == ref["rebuilds"]
