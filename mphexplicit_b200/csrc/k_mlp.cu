@@ -98,19 +98,28 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 }
 __device__ __forceinline__ float lo_bf(uint32_t p) { return __uint_as_float(p << 16); }
 
-// SiLU of two BF16 activations at once, h = z * (1 + tanh(z/2)) / 2 in packed
-// BF16 arithmetic: z/2 (exact), the hardware's packed tanh approximation,
-// s = bf16(t/2 + 1/2), h = bf16(z * s).  One special-function operation per
-// two activations (the FP32 form takes one each, and that pipe bounds the
-// epilogues); the forward passes of training and inference both use it.
-__device__ __forceinline__ uint32_t silu2(uint32_t z2) {
-    const uint32_t half2 = 0x3F003F00u;  // (0.5, 0.5) in BF16
-    uint32_t hz, t, sg, h;
-    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(hz) : "r"(z2), "r"(half2));
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hz));
-    asm("fma.rn.bf16x2 %0, %1, %2, %2;" : "=r"(sg) : "r"(t), "r"(half2));
-    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(h) : "r"(z2), "r"(sg));
+// SiLU in packed BF16 from the half pre-activation hz = z/2:
+//   h = z * sigmoid(z) = z * (1 + tanh(z/2)) / 2 = hz + hz * tanh(hz),
+// one special-function operation (the packed tanh) and one FMA per two
+// activations; the forward passes of training and inference both use it.
+__device__ __forceinline__ uint32_t silu_half2(uint32_t hz2) {
+    uint32_t t, h;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(hz2));
+    asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(hz2), "r"(t));
     return h;
+}
+// The same from z (z/2 is exact in BF16).
+__device__ __forceinline__ uint32_t silu2(uint32_t z2) {
+    uint32_t hz;
+    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(hz) : "r"(z2), "r"(0x3F003F00u));
+    return silu_half2(hz);
+}
+// Two FP32 values to BF16, rounded to nearest (ties away from zero: the
+// conversion instruction rounds ties to even; they differ only on exact ties),
+// with one integer add each and one byte permute: the conversion instruction
+// shares its pipe with the packed tanh, which bounds the hidden-layer epilogues.
+__device__ __forceinline__ uint32_t pack2_near(float a, float b) {
+    return __byte_perm(__float_as_uint(a) + 0x8000u, __float_as_uint(b) + 0x8000u, 0x7632);
 }
 __device__ __forceinline__ float hi_bf(uint32_t p) { return __uint_as_float(p & 0xFFFF0000u); }
 
@@ -145,10 +154,11 @@ __device__ __forceinline__ void store_x(uint8_t* sx, int e, const float* f) {
     st_row16(sx, e, 0, KIN, p);
 }
 
-// forward epilogue of a hidden layer: Z = D + b -> (bf16) zbuf, H = silu(Z) -> hbuf,
-// columns [16 c0, 16 c1) of row e
-__device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias, uint8_t* zbuf, uint8_t* hbuf, int e,
-                                           int c0 = 0, int c1 = H / 16) {
+// forward epilogue of a hidden layer, columns [16 c0, 16 c1) of row e:
+// hz = (D + b) / 2 = D / 2 + bias_half (one FMA, exact scaling), rounded to BF16;
+// H = silu(Z) -> hbuf and, for training, Z = 2 hz (exact) -> zbuf
+__device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias_half, uint8_t* zbuf, uint8_t* hbuf,
+                                           int e, int c0 = 0, int c1 = H / 16) {
 #pragma unroll 1
     for (int c = c0; c < c1; ++c) {
         float v[16];
@@ -156,12 +166,20 @@ __device__ __forceinline__ void epi_hidden(uint32_t trow, const float* bias, uin
         uint32_t zp[8], hp[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            zp[j] = pack2(v[2 * j] + bias[16 * c + 2 * j], v[2 * j + 1] + bias[16 * c + 2 * j + 1]);
-            hp[j] = silu2(zp[j]);
+            const uint32_t hz = pack2_near(fmaf(v[2 * j], 0.5f, bias_half[16 * c + 2 * j]),
+                                           fmaf(v[2 * j + 1], 0.5f, bias_half[16 * c + 2 * j + 1]));
+            hp[j] = silu_half2(hz);
+            if (zbuf) asm("add.rn.bf16x2 %0, %1, %1;" : "=r"(zp[j]) : "r"(hz));
         }
         if (zbuf) st_row16(zbuf, e, 16 * c, H, zp);
         st_row16(hbuf, e, 16 * c, H, hp);
     }
+}
+
+// The hidden layers' biases halved in place in a CTA's copy of the weight
+// image (epi_hidden takes b/2); call between two CTA-wide barriers.
+__device__ __forceinline__ void halve_hidden_biases(float* b1) {
+    for (int k = threadIdx.x; k < 3 * H; k += blockDim.x) b1[k] *= 0.5f;
 }
 
 // backward epilogue: dZ = dH * silu'(Z) in place of Z; optionally H_prev = silu(Z_prev)
@@ -208,6 +226,8 @@ k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ sample
         const uint32_t one2 = 0x3F803F80u;  // two bf16 ones
         for (int k = tid; k < KOUT * TILE * 2 / 16; k += 128) o[k] = make_uint4(one2, one2, one2, one2);
     }
+    __syncthreads();  // the image is in shared memory
+    halve_hidden_biases(reinterpret_cast<float*>(sm + S_W + PK_B));  // ordered by the barrier below
     const float* b1 = reinterpret_cast<const float*>(sm + S_W + PK_B);
     const float* b2 = b1 + H;
     const float* b3 = b2 + H;
@@ -428,6 +448,8 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
         uint4* dst = reinterpret_cast<uint4*>(sm + S_W);
         for (int k = tid; k < PK_BYTES / 16; k += blockDim.x) dst[k] = src[k];
     }
+    __syncthreads();  // the image is in shared memory
+    halve_hidden_biases(reinterpret_cast<float*>(sm + S_W + PK_B));  // ordered by the barrier below
     const float* b1 = reinterpret_cast<const float*>(sm + S_W + PK_B);
     const float* b2 = b1 + H;
     const float* b3 = b2 + H;

@@ -5,7 +5,7 @@ library).
 The network has no reference counterpart (the reference has no learned
 terms); this is a restatement of the same arithmetic in numpy.  `forward` /
 `gradient` with bf16=True round to BF16 where the kernels do (inputs,
-weights, Z = pre-activation, H = SiLU(Z) at the three rounding points of the
+weights, Z = pre-activation, H = SiLU(Z) at the rounding points of the
 kernels' packed form, dY, dZ) and accumulate in FP64 (the
 kernels accumulate in FP32 on the tensor cores); with bf16=False everything is
 FP64, which `tests/` checks against finite differences.
@@ -82,10 +82,10 @@ def _dsilu(z):
 
 def _silu_bf16x2(z):
     """SiLU with the rounding points of the kernels' packed BF16 form (z is
-    already BF16): t = bf16(tanh(z/2)), s = bf16(t/2 + 1/2), h = bf16(z s)."""
-    t = bf16(np.tanh(0.5 * z).astype(np.float32)).astype(np.float64)
-    s = bf16((0.5 * t + 0.5).astype(np.float32)).astype(np.float64)
-    return bf16((z * s).astype(np.float32)).astype(np.float64)
+    already BF16): hz = z/2 (exact), t = bf16(tanh(hz)), h = bf16(hz + hz t)."""
+    hz = 0.5 * z
+    t = bf16(np.tanh(hz).astype(np.float32)).astype(np.float64)
+    return bf16((hz + hz * t).astype(np.float32)).astype(np.float64)
 
 
 def _round(a, on):
