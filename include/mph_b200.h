@@ -374,8 +374,9 @@ int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);
 /* ---- batched form: many independent scenes in one step -----------------
  * No counterpart in the reference, which runs one scene per process; each
  * scene here takes the reference's step (main.cpp:386-431, the start-up sort
- * of main.cpp:357-359 included) with the mixed form's FP32 pair arithmetic
- * and FP64 integration.  All scenes of a batch have the same dimension; walls
+ * of main.cpp:357-359 included) with the pair arithmetic of
+ * MPH_MODE_MIXED_P64 (FP64 density pairs, FP32 force pairs) and FP64
+ * integration.  All scenes of a batch have the same dimension; walls
  * must be static (zero Wall2/3 Velocity and Omega).  Scene s keeps its own
  * *.data parameters, domain and cell grid; a step advances every scene by its
  * own dt.  The sweeps are persistent kernels over (scene, cell tile) work

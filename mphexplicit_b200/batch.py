@@ -2,8 +2,9 @@
 
 A thin host mirror of the mph_batch_* C ABI (include/mph_b200.h).  Every
 scene keeps its own *.data parameters, *.grid particles and cell grid; one
-``step`` advances all of them by their own dt with the mixed form's FP32
-pair arithmetic and FP64 integration, as persistent (scene, cell tile) sweeps
+``step`` advances all of them by their own dt with the pair arithmetic of
+MPH_MODE_MIXED_P64 (FP64 density pairs, FP32 force pairs) and FP64
+integration, as persistent (scene, cell tile) sweeps
 replayed through CUDA graphs.  ``autotune`` picks the tile shape on the batch
 itself without advancing it.
 """

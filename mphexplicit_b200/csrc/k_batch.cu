@@ -21,9 +21,11 @@
 // evaluates the tile's pairs from there; no neighbour list is stored.  Staged
 // positions are tile-relative, split into a part on a power-of-two grid and
 // an FP32 remainder, so x_j - x_i is the true displacement rounded once to
-// FP32.  Pair arithmetic is FP32 with the mixed form's formulas
-// (Kahan-compensated sums for the short-range pairs); positions and
-// velocities are integrated in FP64.  A tile whose halo does not fit in
+// FP32.  The density sweep's DensityP / DivergenceP pairs are evaluated in
+// FP64 on that displacement (the pressure is a bulk modulus times a small
+// difference of two numbers near N0p), every other pair term in FP32 with
+// the mixed form's formulas (Kahan-compensated short-range force sums);
+// positions and velocities are integrated in FP64.  A tile whose halo does not fit in
 // shared memory is split in two until it does.  mph_batch_step replays K steps
 // as one CUDA graph; mph_batch_autotune times the candidate tile shapes on the
 // batch itself and keeps the fastest.
@@ -57,9 +59,11 @@ struct alignas(16) BScene {
     int has_st, ratio_all_one, uniform_mu, pad0;
     double dmin[3], width[3], inv_width[3], cell_width[3], half_width[3];
     double dt, shift_thr, grid, inv_grid, vol_d, n0p_d;
+    double rp2_d, inv_rp_d, cp_d, cp_m2_d;  // FP64 density pairs
     double gravity[3];
     double density[MPH_TYPE_COUNT], bulk_modulus_d[MPH_TYPE_COUNT], bulk_viscosity_d[MPH_TYPE_COUNT];
     float cut2_a, cut2_b, short_r2;
+    float rp2_pre;                      // RP^2 a little widened: FP32 pre-filter of the FP64 density pairs
     float ra2, rp2, rv2, rg2;
     float inv_ra, inv_rp, inv_rv, inv_rg;
     float ca, cp, cg, cv;
@@ -493,19 +497,38 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                     }
                 };
                 if (SWEEP == 0) {
-                    float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
+                    double spd = 0.0, sdd = 0.0;  // DensityP, DivergenceP: FP64 pairs
                     float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
                     for_near(sc.cut2_a, [&](int j, float dx, float dy, float dz, float r2) {
                             const float rinv = rsqrt_nr(r2);
                             const float rr = r2 * rinv;
-                            if (r2 <= sc.rp2) {
-                                const float q = 1.0f - rr * sc.inv_rp;
-                                kahan_add(sp, cpk, sc.cp * q * q);  // wp
-                                const float dw = sc.cp_m2 * q;     // dwpdr
-                                const float4 vj = sV[j];
-                                float ue = (vj.x - vi.x) * dx + (vj.y - vi.y) * dy;
-                                if (DIM == 3) ue += (vj.z - vi.z) * dz;
-                                kahan_add(sd, cdk, -(ue * rinv) * dw);
+                            if (r2 <= sc.rp2_pre) {
+                                // FP64 displacement: the hi parts' difference is exact in FP32,
+                                // the lo parts carry the rest
+                                const float4 pj = sP[j];
+                                double dd[3];
+                                if (DIM == 2) {
+                                    dd[0] = (double)(pj.x - pi.x) + ((double)pj.z - (double)pi.z);
+                                    dd[1] = (double)(pj.y - pi.y) + ((double)pj.w - (double)pi.w);
+                                    dd[2] = 0.0;
+                                } else {
+                                    const float4 lj = sL[j];
+                                    dd[0] = (double)(pj.x - pi.x) + ((double)lj.x - (double)li.x);
+                                    dd[1] = (double)(pj.y - pi.y) + ((double)lj.y - (double)li.y);
+                                    dd[2] = (double)(pj.z - pi.z) + ((double)lj.z - (double)li.z);
+                                }
+                                const double r2d = dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2];
+                                if (r2d <= sc.rp2_d) {
+                                    const double y = rsqrt_dnr(r2d);
+                                    const double q = 1.0 - r2d * y * sc.inv_rp_d;
+                                    spd += sc.cp_d * q * q;  // wp
+                                    const double dw = sc.cp_m2_d * q;
+                                    const float4 vj = sV[j];
+                                    double ue = ((double)vj.x - (double)vi.x) * dd[0] +
+                                                ((double)vj.y - (double)vi.y) * dd[1];
+                                    if (DIM == 3) ue += ((double)vj.z - (double)vi.z) * dd[2];
+                                    sdd -= ue * y * dw;
+                                }
                             }
                             if (ST && st) {
                                 const int tj = type_of(j);
@@ -513,9 +536,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_bt_sweep(BatchDev b) {
                                 else st_density<true>(sc, ti, tj, r2, rr, dx, dy, dz, sa, cak, g0, g1, g2);
                             }
                     });
-                    // the compensated sums keep their low parts; N0p is subtracted in FP64
-                    const double strain = ((double)sp - (double)cpk) - sc.n0p_d;
-                    const double div = (double)sd - (double)cdk;
+                    const double strain = spd - sc.n0p_d;
+                    const double div = sdd;
                     double kappa = sc.bulk_modulus_d[ti];
                     if (strain < 0.0) kappa = 0.0;
                     const double pp = -sc.bulk_viscosity_d[ti] * div + kappa * strain;
@@ -704,7 +726,7 @@ extern "C" void mph_batch_destroy(mph_batch* b) {
     delete b;
 }
 
-// FP32 pair constants of one scene (the mixed form's, from the FP64 values).
+// Pair constants of one scene (the mixed form's, from the FP64 values).
 static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& k) {
     std::memset(&s, 0, sizeof(s));
     s.n = c.n;
@@ -745,8 +767,10 @@ static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& 
     s.rv2 = (float)c.rv2;
     s.rg2 = (float)c.rg2;
     // the density sums take r^2 <= R^2 (main.cpp:1684), the forces r^2 < R^2:
-    // pairs are selected by r^2 < cut2, so cut2_a is the next float above
-    s.cut2_a = std::nextafter(c.has_st ? std::max(s.rp2, std::max(s.ra2, s.rg2)) : s.rp2, INFINITY);
+    // pairs are selected by r^2 < cut2 in FP32, so cut2_a lies a little above
+    // (the FP64 test r^2 <= RP^2 decides the pressure pairs)
+    s.rp2_pre = (float)(c.rp2 * (1.0 + 1e-5));
+    s.cut2_a = std::nextafter(c.has_st ? std::max(s.rp2_pre, std::max(s.ra2, s.rg2)) : s.rp2_pre, INFINITY);
     s.cut2_b = std::max(s.rp2, s.rv2);
     if (c.has_st) s.cut2_b = std::max(s.cut2_b, std::max(s.ra2, s.rg2));
     s.inv_ra = (float)(1.0 / c.ra);
@@ -769,6 +793,10 @@ static void fill_bscene(BScene& s, const mph::SimConst& c, const mph_constants& 
     s.n0a = (float)c.n0a;
     s.n0p = (float)c.n0p;
     s.n0p_d = c.n0p;
+    s.rp2_d = c.rp2;
+    s.inv_rp_d = 1.0 / c.rp;
+    s.cp_d = c.cp;
+    s.cp_m2_d = c.cp * c.m2_rp;
     s.inv_r2g_rg = (float)(c.rg / c.r2g);
     s.l0 = (float)c.l0;
 }

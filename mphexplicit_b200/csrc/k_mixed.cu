@@ -365,13 +365,6 @@ __device__ __forceinline__ void load_tables(const MixConst& m, SharedTables& t) 
     __syncthreads();
 }
 
-// 1/sqrt from an FP32 seed plus one Newton step (relative error ~1e-14), for
-// the FP64 density pairs.
-__device__ __forceinline__ double rsqrt64(double r2) {
-    const double y = (double)rsqrtf((float)r2);
-    return y * (1.5 - 0.5 * r2 * y * y);
-}
-
 // Sweep A: DensityP and DivergenceP over the short part of the list with the
 // exact FP32 displacement (S64: pair arithmetic in FP64, the displacement
 // assembled in FP64 from the hi/lo parts, FP32 velocities), plus, with
@@ -418,7 +411,7 @@ k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v
             const double dzd = (double)((pj.z - pi.z) + dh.z) + (((double)lj.z - (double)li.z) + (double)dl.z);
             const double r2d = dxd * dxd + dyd * dyd + dzd * dzd;
             if (r2d <= c.rp2) {
-                const double y = rsqrt64(r2d);
+                const double y = rsqrt_dnr(r2d);
                 const double q = 1.0 - r2d * y * m.inv_rp_d;
                 spd += m.cp_d * q * q;
                 const double dw = m.cp_m2_d * q;
