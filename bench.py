@@ -131,7 +131,7 @@ def measure_learned(args, rank):
     """The learned form on the 1 M-fluid dam break (80x80x160 fluid in a
     240x80x192-cell box): training data from the FP64 step on 8 seeded
     jitters (2000 FP64 steps in all, spread over the first ~1100 steps of the
-    flow by an untimed pre-roll in the FP64-core mixed form), Adam training of
+    flow by an untimed pre-roll in MPH_MODE_MIXED_P64), Adam training of
     the edge MLP on the tensor cores, then a timed run of `learned_steps`
     steps with the plain FP64 step as judge every 20 steps (fallback above a
     relative force error of 1e-2), and its velocity error against the FP64 run
@@ -470,7 +470,7 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
            "vel": vel, "fluid": fluid}
     # roofline of the dominant kernel: algorithmic bytes per particle the
     # kernel updates (FP64 state, neighbour re-reads on chip) over its time per
-    # step (the FP64-core force sweep is two launches per step: both count)
+    # step (every launch of that kernel in the step counts)
     name, (nl, tot_ms) = max(prof.items(), key=lambda kv: kv[1][1])
     avg_s = tot_ms / args.steps / 1e3
     peak, peak_kind = measured_peaks()

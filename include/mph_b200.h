@@ -211,9 +211,29 @@ int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long long ind_capa
 int mph_compute_virial(mph_ctx* ctx);
 
 /* Output files in the reference formats and in sorted order:
- * writeVtkFile (main.cpp:698-834) and writeProfFile (main.cpp:672-696). */
+ * writeVtkFile (main.cpp:698-834) and writeProfFile (main.cpp:672-696),
+ * byte for byte.  The device formats every particle's lines ("%e" exact to
+ * the last digit, as glibc prints it); the host copies the text out and writes
+ * it.  These two return once the file is written. */
 int mph_write_vtk(mph_ctx* ctx, const char* path);
 int mph_write_prof(mph_ctx* ctx, const char* path);
+
+/* The same files written behind the step: the state at the call is
+ * formatted on the context's stream (ordered before any later mph_step), and a
+ * writer thread of the context copies it out and writes the file while the
+ * caller steps on.  Two documents can be in flight; a third call waits for the
+ * first one's copy.  mph_output_wait returns once every file is written, with
+ * the first write failure since the previous wait; mph_destroy also waits. */
+int mph_write_vtk_async(mph_ctx* ctx, const char* path);
+int mph_write_prof_async(mph_ctx* ctx, const char* path);
+int mph_output_wait(mph_ctx* ctx);
+
+/* The device formatter on its own: values[0..n) as "%e\n" lines, each value
+ * first cast to float when as_float (writeVtkFile's "(float)" fields), into
+ * out[0..capacity); *length = bytes written.  MPH_ERR_CAPACITY if out is too
+ * small (at most 15 bytes per value). */
+int mph_format_e(const double* values, long long n, int as_float, char* out, long long capacity,
+                 long long* length);
 
 /* writeVtkFile (main.cpp:698-834) from caller host arrays of n particles
  * (no context needed): same text, same field order, same float casts. */

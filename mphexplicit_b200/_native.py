@@ -179,6 +179,10 @@ SIGNATURES = {
     "mph_compute_virial": (_I, [_P]),
     "mph_write_vtk": (_I, [_P, C.c_char_p]),
     "mph_write_prof": (_I, [_P, C.c_char_p]),
+    "mph_write_vtk_async": (_I, [_P, C.c_char_p]),
+    "mph_write_prof_async": (_I, [_P, C.c_char_p]),
+    "mph_output_wait": (_I, [_P]),
+    "mph_format_e": (_I, [C.c_void_p, C.c_longlong, _I, C.c_char_p, C.c_longlong, C.POINTER(C.c_longlong)]),
     "mph_write_vtk_arrays": (_I, [C.c_char_p, _I, _ip, _dp, _dp, _dp, _ip, _dp, _dp, _dp]),
     "mph_conserved_sums": (_I, [_P, _dp]),
     "mph_write_checkpoint": (_I, [_P, C.c_char_p]),

@@ -30,13 +30,9 @@ namespace {
 constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 
 // Resident 128-thread blocks per SM the force sweep is compiled for (register
-// cap 65536 / (128 * blocks)), and pairs of its long-range loop whose gathers
-// are issued together; set by measurement on the full dam break.
+// cap 65536 / (128 * blocks)); set by measurement on the full dam break.
 #ifndef MPH_MIXB_MINB_FUSED
 #define MPH_MIXB_MINB_FUSED 8
-#endif
-#ifndef MPH_MIXB_BATCH_FUSED
-#define MPH_MIXB_BATCH_FUSED 4
 #endif
 
 struct MixConst {

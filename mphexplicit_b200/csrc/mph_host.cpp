@@ -22,6 +22,7 @@
 #include "mph_io.h"
 #include "mph_mixed.h"
 #include "mph_learned.h"
+#include "mph_text.h"
 
 using mph::SimConst;
 using mph::StepScalars;
@@ -83,6 +84,7 @@ struct mph_ctx {
     long long launches = 0;
     Profiler prof;
     std::string err;
+    mph::TextWriter* text = nullptr;  // *.prof / *.vtk writer thread, made by the first write
 };
 
 static thread_local std::string g_err;
@@ -480,6 +482,7 @@ static int validate_inputs(int n, const int* type, const double* xyz, const doub
 
 extern "C" void mph_destroy(mph_ctx* ctx) {
     if (!ctx) return;
+    delete ctx->text;  // finishes the files still being written
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_fp64(ctx->d);
     for (auto& q : ctx->prof.pending) { cudaEventDestroy(q.a); cudaEventDestroy(q.b); }
@@ -1046,17 +1049,82 @@ extern "C" int mph_compute_virial(mph_ctx* ctx) {
     return MPH_OK;
 }
 
-extern "C" int mph_write_vtk(mph_ctx* ctx, const char* path) {
-    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
-    const size_t n = (size_t)ctx->n;
-    std::vector<int> type(n), nc(n);
-    std::vector<double> x(3 * n), v(3 * n), f(3 * n), da(n), sp(n), vp(n);
-    TRY(mph_get_state(ctx, nullptr, type.data(), x.data(), v.data(), f.data(), nc.data(), da.data(), sp.data(),
-                      vp.data()));
-    const int st = mph::write_vtk_host(path, ctx->n, type.data(), x.data(), v.data(), f.data(), nc.data(), da.data(),
-                                       sp.data(), vp.data());
-    if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
+// ---- output files, formatted on the device ----------------------------------
+static int text_submit(mph_ctx* ctx, mph::TextDoc& doc, const char* path, const char* what) {
+    if (!ctx->text) {
+        int dev = 0;
+        CUDA_TRY(ctx, cudaGetDevice(&dev));
+        ctx->text = new mph::TextWriter(dev);
+    }
+    std::string err;
+    Launch L(ctx, what);
+    const int st = ctx->text->submit(doc, ctx->stream, path, &err, &L.count);
+    if (st != MPH_OK) return fail(ctx, st, err);
     return MPH_OK;
+}
+
+// writeVtkFile (main.cpp:698-834): the same sections, each particle's lines
+// formatted by the device in the context's (cell-sorted) order.
+extern "C" int mph_write_vtk_async(mph_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    TRY(sync_state(ctx));
+    mph::DevFP64& d = ctx->d;
+    const int n = ctx->n;
+    char h[256];
+    mph::TextDoc doc;
+    doc.nsec = doc.nblocks = doc.head_used = 0;
+    bool ok = true;
+    std::snprintf(h, sizeof(h),
+                  "# vtk DataFile Version 2.0\nUnstructured Grid Example\nASCII\nDATASET UNSTRUCTURED_GRID\n"
+                  "POINTS %d float\n", n);
+    ok &= mph::text_add(doc, h, mph::kRecVec3f, n, d.pos[d.cur]);
+    std::snprintf(h, sizeof(h), "CELLS %d %d\n", n, 2 * n);
+    ok &= mph::text_add(doc, h, mph::kRecCell, n);
+    std::snprintf(h, sizeof(h), "\nCELL_TYPES %d\n", n);
+    ok &= mph::text_add(doc, h, mph::kRecOne, n);
+    std::snprintf(h, sizeof(h), "\n\nPOINT_DATA %d\nSCALARS label float 1\nLOOKUP_TABLE default\n", n);
+    ok &= mph::text_add(doc, h, mph::kRecInt, n, d.type[d.cur]);
+    ok &= mph::text_add(doc, "\nSCALARS DensityA float 1\nLOOKUP_TABLE default\n", mph::kRecScalarf, n, d.dens_a);
+    ok &= mph::text_add(doc, "\nSCALARS VolStrainP float 1\nLOOKUP_TABLE default\n", mph::kRecScalarf, n,
+                        d.strain_p);
+    ok &= mph::text_add(doc, "\nSCALARS VirialPressureAtParticle float 1\nLOOKUP_TABLE default\n",
+                        mph::kRecScalarf, n, d.virial_p);
+    ok &= mph::text_add(doc, "\nSCALARS neighbor float 1\nLOOKUP_TABLE default\n", mph::kRecInt, n, d.ncount);
+    ok &= mph::text_add(doc, "\nVECTORS velocity float\n", mph::kRecVec3f, n, d.vel[d.vcur]);
+    ok &= mph::text_add(doc, "\nVECTORS force float\n", mph::kRecVec3f, n, d.force);
+    ok &= mph::text_add(doc, "\n", mph::kRecNone, 0);
+    if (!ok) return fail(ctx, MPH_ERR_STATE, "vtk document does not fit its tables");
+    return text_submit(ctx, doc, path, "text_vtk");
+}
+
+// writeProfFile (main.cpp:672-696), formatted by the device.
+extern "C" int mph_write_prof_async(mph_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    mph::DevFP64& d = ctx->d;
+    const mph_grid_header& g = ctx->h;
+    char h[256];
+    std::snprintf(h, sizeof(h), "%e\n%d %e %e %e %e %e %e %e\n", ctx->time, g.particle_count, g.particle_spacing,
+                  g.domain_min[0], g.domain_max[0], g.domain_min[1], g.domain_max[1], g.domain_min[2],
+                  g.domain_max[2]);
+    mph::TextDoc doc;
+    doc.nsec = doc.nblocks = doc.head_used = 0;
+    if (!mph::text_add(doc, h, mph::kRecProf, ctx->n, d.pos[d.cur], d.vel[d.vcur], d.type[d.cur]))
+        return fail(ctx, MPH_ERR_STATE, "prof document does not fit its tables");
+    return text_submit(ctx, doc, path, "text_prof");
+}
+
+extern "C" int mph_output_wait(mph_ctx* ctx) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    if (!ctx->text) return MPH_OK;
+    std::string err;
+    const int st = ctx->text->wait(&err);
+    if (st != MPH_OK) return fail(ctx, st, err);
+    return MPH_OK;
+}
+
+extern "C" int mph_write_vtk(mph_ctx* ctx, const char* path) {
+    TRY(mph_write_vtk_async(ctx, path));
+    return mph_output_wait(ctx);
 }
 
 extern "C" int mph_write_vtk_arrays(const char* path, int n, const int* type, const double* xyz, const double* vel,
@@ -1072,16 +1140,8 @@ extern "C" int mph_write_vtk_arrays(const char* path, int n, const int* type, co
 }
 
 extern "C" int mph_write_prof(mph_ctx* ctx, const char* path) {
-    if (!ctx || !path) return fail(ctx, MPH_ERR_ARG, "bad arguments");
-    const size_t n = (size_t)ctx->n;
-    std::vector<int> type(n);
-    std::vector<double> x(3 * n), v(3 * n);
-    TRY(mph_get_state(ctx, nullptr, type.data(), x.data(), v.data(), nullptr, nullptr, nullptr, nullptr, nullptr));
-    mph_grid_header h = ctx->h;
-    h.time = ctx->time;
-    const int st = mph_write_grid_file(path, &h, type.data(), x.data(), v.data());
-    if (st != MPH_OK) return fail(ctx, st, std::string("cannot write ") + path);
-    return MPH_OK;
+    TRY(mph_write_prof_async(ctx, path));
+    return mph_output_wait(ctx);
 }
 
 extern "C" int mph_write_checkpoint(mph_ctx* ctx, const char* path) {

@@ -115,6 +115,17 @@ def write_vtk_arrays(path: str, state: dict) -> None:
                                          _dp(f64["vol_strain_p"]), _dp(f64["virial_pressure"])))
 
 
+def format_e(values, as_float: bool = False) -> bytes:
+    """values as "%e\\n" lines, formatted by the device (each value cast to
+    float first when as_float, as writeVtkFile prints its fields)."""
+    v = np.ascontiguousarray(values, np.float64).ravel()
+    cap = 15 * len(v)
+    out = C.create_string_buffer(max(cap, 1))
+    n = C.c_longlong(0)
+    _check(N.load().mph_format_e(v.ctypes.data_as(C.c_void_p), len(v), int(bool(as_float)), out, cap, C.byref(n)))
+    return out.raw[:n.value]
+
+
 @dataclass
 class Checkpoint:
     """Contents of an exact checkpoint (mph_write_checkpoint): the particles in
@@ -321,6 +332,18 @@ class Solver:
     def write_prof(self, path: str) -> None:
         _check(self._lib.mph_write_prof(self._ctx, str(path).encode()), self._ctx)
 
+    def write_vtk_async(self, path: str) -> None:
+        """Formats the current state on the device and writes the file from
+        the context's writer thread while stepping continues."""
+        _check(self._lib.mph_write_vtk_async(self._ctx, str(path).encode()), self._ctx)
+
+    def write_prof_async(self, path: str) -> None:
+        _check(self._lib.mph_write_prof_async(self._ctx, str(path).encode()), self._ctx)
+
+    def output_wait(self) -> None:
+        """Returns once every file written behind the step is on disk."""
+        _check(self._lib.mph_output_wait(self._ctx), self._ctx)
+
     def close(self) -> None:
         if getattr(self, "_ctx", None):
             self._lib.mph_destroy(self._ctx)
@@ -357,7 +380,7 @@ def run(data: str, grid: str, prof: str = "sample%03d.prof", vtk: str = "sample%
     lines = []
     while t < params.end_time + 1.0e-5 * dt:
         if t + 1.0e-5 * dt >= out_next:
-            s.write_prof(prof % istep)
+            s.write_prof_async(prof % istep)
             lines.append("@ Prof Output Time : %e" % t)
             out_next += params.output_interval
         a = _time.perf_counter()
@@ -368,11 +391,12 @@ def run(data: str, grid: str, prof: str = "sample%03d.prof", vtk: str = "sample%
         if t + 1.0e-5 * dt >= vtk_next:
             if mode == "fp64":
                 s.compute_virial()
-            s.write_vtk(vtk % istep)
+            s.write_vtk_async(vtk % istep)
             lines.append("@ Vtk Output Time : %e" % t)
             vtk_next += params.vtk_output_interval
         t += dt
         istep += 1
+    s.output_wait()
     info = s.info()
     s.close()
     if log:
