@@ -13,7 +13,7 @@ value = fluid particles x steps / seconds, summed over ranks (replicas: the
 step does not shard, each rank runs its own scene on its own GPU).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp64|mixed|mixed_p64] [--only]
-                  [--forms fp64,mixed,mixed_p64,learned,batch,two_fluid]
+                  [--forms fp64,mixed,mixed_p64,learned,batch,two_fluid,output]
   python bench.py --impl reference ...   # the reference's own CPU step, all host threads
 
 One JSON line on rank 0.
@@ -371,6 +371,71 @@ def measure_two_fluid(args, rank):
     return out
 
 
+def measure_output(args, sc, rank):
+    """The output path (writeVtkFile / writeProfFile, main.cpp:672-834) on the
+    benchmark scene after 20 MPH_MODE_MIXED_P64 steps: the device formatting
+    time per document (CUDA events on the context's stream, 3 launches each),
+    mph_write_vtk / mph_write_prof end to end (wall clock: format, copy out,
+    fwrite into the page cache), the host printf writer on the same state
+    (the reference's writer), whether the bytes agree, and the stepping time
+    with a VTK written behind every `output_every` steps against none."""
+    import tempfile
+    import time
+    import mphexplicit_b200 as M
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode="mixed_p64")
+    s.step(20)
+    s.synchronize()
+    out = {"workload": workload_name(sc), "particles": sc.n}
+    with tempfile.TemporaryDirectory() as td:
+        vtk, prof, host = (os.path.join(td, f) for f in ("d.vtk", "d.prof", "h.vtk"))
+        s.write_vtk(vtk)  # warm-up: buffers, writer thread
+        s.write_prof(prof)
+        s.profile(True)
+        tv, tp = [], []
+        for _ in range(3):
+            a = time.perf_counter()
+            s.write_vtk(vtk)
+            tv.append(time.perf_counter() - a)
+            a = time.perf_counter()
+            s.write_prof(prof)
+            tp.append(time.perf_counter() - a)
+        p = s.profile_read()
+        s.profile(False)
+        vtk_bytes, prof_bytes = os.path.getsize(vtk), os.path.getsize(prof)
+        st = s.state()
+        a = time.perf_counter()
+        M.write_vtk_arrays(host, st)
+        host_s = time.perf_counter() - a
+        same = open(host, "rb").read() == open(vtk, "rb").read()
+        ms_vtk = p["text_vtk"][1] / 3
+        ms_prof = p["text_prof"][1] / 3
+        # VTK record inputs: pos, vel, force (double4), type, NeighborCount (int),
+        # DensityA, VolStrainP, VirialPressure (double) = 128 B per particle
+        out.update({"vtk_bytes": vtk_bytes, "prof_bytes": prof_bytes,
+                    "vtk_device_ms": ms_vtk, "prof_device_ms": ms_prof,
+                    "vtk_device_gbs": (vtk_bytes + 128.0 * sc.n) / (ms_vtk / 1e3) / 1e9,
+                    "write_vtk_s": min(tv), "write_prof_s": min(tp), "host_printf_vtk_s": host_s,
+                    "write_vtk_speedup_vs_host": host_s / min(tv), "bytes_equal_host": same})
+        every, files = args.output_every, args.output_files
+        s.synchronize()
+        a = time.perf_counter()
+        s.step(every * files)
+        s.synchronize()
+        base = time.perf_counter() - a
+        a = time.perf_counter()
+        for k in range(files):
+            s.step(every)
+            s.write_vtk_async(os.path.join(td, "a%d.vtk" % (k % 2)))
+        s.synchronize()
+        stepped = time.perf_counter() - a
+        s.output_wait()
+        done = time.perf_counter() - a
+        out.update({"output_every": every, "files": files, "steps_s_no_output": base,
+                    "steps_s_with_output_behind": stepped, "all_files_written_s": done})
+    s.close()
+    return out
+
+
 def make_scene(args, rank):
     from mphexplicit_b200 import scenes
     if args.scene == "dam":
@@ -521,13 +586,15 @@ def main():
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch,two_fluid",
+    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch,two_fluid,output",
                     help="forms to measure (comma list); the headline --mode must be among them for a full line")
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
     ap.add_argument("--learn-epochs", type=int, default=4)
     ap.add_argument("--batch-steps", type=int, default=2000)
+    ap.add_argument("--output-every", type=int, default=100, help="steps between VTK files written behind the step")
+    ap.add_argument("--output-files", type=int, default=5)
     ap.add_argument("--two-fluid-n", type=int, default=200, help="fluid particles per axis of the two-fluid column")
     ap.add_argument("--two-fluid-steps", type=int, default=50)
     ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
@@ -581,6 +648,8 @@ def main():
         forms["batch"] = measure_batch(args, rank)
     if "two_fluid" in wanted:
         forms["two_fluid"] = measure_two_fluid(args, rank)
+    if "output" in wanted:
+        forms["output"] = measure_output(args, sc, rank)
     if args.mode not in res:  # a run of the extra forms alone (profiling)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "unit": UNIT, "n_gpus": world, "forms": forms}), flush=True)

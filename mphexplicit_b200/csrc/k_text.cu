@@ -4,9 +4,10 @@
 // (writeProfFile, main.cpp:672-696; writeVtkFile, main.cpp:698-834).  Here a
 // document is a list of sections, each a header string followed by one
 // record per particle; three launches turn it into the file's bytes in device
-// memory: (1) every record's length, summed per block; (2) one block scans the
-// block sums into byte offsets; (3) every record is formatted again and
-// stored at its offset.  The host then copies the bytes out and writes them
+// memory: (1) every record's length (from the value's sign and magnitude, no
+// digits), summed per block; (2) one block scans the block sums into byte
+// offsets; (3) every record is formatted into shared memory at its offset and
+// the block's text is stored with aligned 16-byte stores.  The host then copies the bytes out and writes them
 // with one fwrite.
 //
 // "%e" is exact: the digits equal glibc's (the decimal value of the double,
@@ -23,7 +24,11 @@
 namespace mph {
 namespace {
 
-constexpr int kTextThreads = 256;  // records per block
+constexpr int kTextThreads = kTextBlockUnits;  // threads per block, one unit each
+// A block's text: at most one header and 255 records, or 256 records, plus
+// the 15-byte alignment lead and one unit of slack.
+constexpr int kTextStageBytes = (kTextMaxUnit + 255 * 103 + 15 + kTextMaxUnit + 15) / 16 * 16;
+static_assert(kTextMaxRecord[kRecProf] == 103, "stage bound assumes the longest record is 103 bytes");
 constexpr int kBigWords = 32;      // 1024-bit integers: the exact path needs < 860 bits
 
 // ---- exact comparison (slow path) ------------------------------------------
@@ -202,6 +207,33 @@ __device__ int fmt_e(char* o, double x) {
 
 __device__ __forceinline__ int fmt_e_float(char* o, double x) { return fmt_e(o, (double)__double2float_rn(x)); }
 
+// Lengths without the digits: "%e" is 12 characters plus the sign while the
+// printed exponent has two digits, which holds for every value in
+// [1.0000001e-99, 9.9e99) and for every float; outside that range the value
+// is formatted to be measured.
+__device__ __forceinline__ int len_e(double x) {
+    const uint64_t bits = (uint64_t)__double_as_longlong(x);
+    const int sign = (int)(bits >> 63);
+    if (((bits >> 52) & 0x7ff) == 0x7ff) return sign + 3;
+    const double ax = fabs(x);
+    if (ax == 0.0 || (ax >= 1.0000001e-99 && ax < 9.9e99)) return sign + 12;
+    char t[16];
+    return fmt_e(t, x);
+}
+
+__device__ __forceinline__ int len_e_float(double x) { return len_e((double)__double2float_rn(x)); }
+
+__device__ __forceinline__ int len_uint(uint32_t v) {
+    int k = 1;
+    while (v >= 10) {
+        v /= 10;
+        ++k;
+    }
+    return k;
+}
+
+__device__ __forceinline__ int len_int(int v) { return v < 0 ? 1 + len_uint(0u - (uint32_t)v) : len_uint((uint32_t)v); }
+
 // ---- records -------------------------------------------------------------------
 // One record of a section: the particle's line in the reference's format.
 __device__ int format_record(const TextSection& s, int i, char* o) {
@@ -265,6 +297,34 @@ __device__ int format_record(const TextSection& s, int i, char* o) {
     return k;
 }
 
+// The length format_record gives, computed without formatting.
+__device__ int record_len(const TextSection& s, int i) {
+    switch (s.kind) {
+        case kRecProf: {
+            const double4 q = reinterpret_cast<const double4*>(s.src0)[i];
+            const double4 v = reinterpret_cast<const double4*>(s.src1)[i];
+            return len_int(reinterpret_cast<const int*>(s.src2)[i]) + len_e(q.x) + len_e(q.y) + len_e(q.z) +
+                   len_e(v.x) + len_e(v.y) + len_e(v.z) + 8;
+        }
+        case kRecVec3f: {
+            const double4 q = reinterpret_cast<const double4*>(s.src0)[i];
+            return len_e_float(q.x) + len_e_float(q.y) + len_e_float(q.z) + 3;
+        }
+        case kRecScalarf:
+            return len_e_float(reinterpret_cast<const double*>(s.src0)[i]) + 1;
+        case kRecScalard:
+            return len_e(reinterpret_cast<const double*>(s.src0)[i]) + 1;
+        case kRecInt:
+            return len_int(reinterpret_cast<const int*>(s.src0)[i]) + 1;
+        case kRecCell:
+            return len_int(i) + 3;
+        case kRecOne:
+            return 2;
+        default:
+            return 0;
+    }
+}
+
 // Unit u of section s: 0 is the header, u >= 1 the record of particle u - 1.
 __device__ __forceinline__ int format_unit(const TextDoc& d, const TextSection& s, int u, char* o) {
     if (u == 0) {
@@ -280,13 +340,19 @@ __device__ __forceinline__ int find_section(const TextDoc& d, int b) {
     return k;
 }
 
+// Pass 1: every unit's length (kept for pass 3) and the block's sum.
 __global__ void __launch_bounds__(kTextThreads) k_text_count(const __grid_constant__ TextDoc d,
+                                                             uint16_t* __restrict__ unit_len,
                                                              uint32_t* __restrict__ blk_bytes) {
     const int b = blockIdx.x;
     const TextSection& s = d.sec[find_section(d, b)];
     const int u = (b - s.first_block) * kTextThreads + threadIdx.x;
-    char buf[kTextMaxUnit];
-    uint32_t len = u <= s.n ? (uint32_t)format_unit(d, s, u, buf) : 0u;
+    uint32_t len = 0;
+    if (u == 0)
+        len = (uint32_t)s.head_len;
+    else if (u <= s.n)
+        len = (uint32_t)record_len(s, u - 1);
+    unit_len[(size_t)b * kTextThreads + threadIdx.x] = (uint16_t)len;
     for (int o = 16; o > 0; o >>= 1) len += __shfl_xor_sync(0xffffffffu, len, o);
     __shared__ uint32_t ws[kTextThreads / 32];
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = len;
@@ -331,31 +397,56 @@ __global__ void __launch_bounds__(1024) k_text_scan(const uint32_t* __restrict__
         if (threadIdx.x == 1023) carry = incl;
         __syncthreads();
     }
-    if (threadIdx.x == 0) off[nblocks] = carry;
+    if (threadIdx.x == 0) {
+        off[nblocks] = carry;
+        off[nblocks + 1] = 0;  // the length-mismatch flag of pass 3
+    }
 }
 
+// Pass 3: every unit formatted into shared memory at its offset within the
+// block, then the block's bytes stored with aligned 16-byte stores (bytes at
+// the two ragged ends).  A unit whose text differs in length from pass 1 sets
+// off[nblocks + 1].
 __global__ void __launch_bounds__(kTextThreads) k_text_write(const __grid_constant__ TextDoc d,
-                                                             const unsigned long long* __restrict__ off,
+                                                             const uint16_t* __restrict__ unit_len,
+                                                             unsigned long long* __restrict__ off,
                                                              char* __restrict__ out) {
+    __shared__ __align__(16) char stage[kTextStageBytes];
+    __shared__ uint32_t ws[kTextThreads / 32];
     const int b = blockIdx.x;
     const TextSection& s = d.sec[find_section(d, b)];
     const int u = (b - s.first_block) * kTextThreads + threadIdx.x;
-    char buf[kTextMaxUnit];
-    const uint32_t len = u <= s.n ? (uint32_t)format_unit(d, s, u, buf) : 0u;
-    // exclusive scan of the lengths within the block
+    const uint32_t len = unit_len[(size_t)b * kTextThreads + threadIdx.x];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t x = len;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
-    __shared__ uint32_t ws[kTextThreads / 32];
     if (lane == 31) ws[w] = x;
     __syncthreads();
-    uint32_t before = 0;
-    for (int k = 0; k < w; ++k) before += ws[k];
-    char* dst = out + off[b] + before + (x - len);
-    for (uint32_t c = 0; c < len; ++c) dst[c] = buf[c];
+    uint32_t before = 0, total = 0;
+    for (int k = 0; k < kTextThreads / 32; ++k) {
+        before += k < w ? ws[k] : 0u;
+        total += ws[k];
+    }
+    const unsigned long long base = off[b];
+    const int a = (int)(base & 15ull);
+    if (u <= s.n) {
+        const int got = format_unit(d, s, u, stage + a + before + (x - len));
+        if (got != (int)len) atomicOr(reinterpret_cast<unsigned int*>(off + d.nblocks + 1), 1u);
+    }
+    __syncthreads();
+    char* g = out + (base - (unsigned long long)a);  // 16-byte aligned
+    const int end = a + (int)total;
+    for (int lo = threadIdx.x * 16; lo < end; lo += kTextThreads * 16) {
+        if (lo >= a && lo + 16 <= end) {
+            *reinterpret_cast<uint4*>(g + lo) = *reinterpret_cast<const uint4*>(stage + lo);
+        } else {
+            const int c1 = lo + 16 < end ? lo + 16 : end;
+            for (int c = lo > a ? lo : a; c < c1; ++c) g[c] = stage[c];
+        }
+    }
 }
 
 // Values as "%e\n" lines (as_float: each cast to float first, as writeVtkFile
@@ -388,11 +479,12 @@ size_t text_max_bytes(const TextDoc& d) {
     return t;
 }
 
-int launch_text(const TextDoc& d, uint32_t* blk_bytes, unsigned long long* off, char* out, cudaStream_t s) {
+int launch_text(const TextDoc& d, uint16_t* unit_len, uint32_t* blk_bytes, unsigned long long* off, char* out,
+                cudaStream_t s) {
     if (d.nblocks <= 0) return 0;
-    k_text_count<<<d.nblocks, kTextThreads, 0, s>>>(d, blk_bytes);
+    k_text_count<<<d.nblocks, kTextThreads, 0, s>>>(d, unit_len, blk_bytes);
     k_text_scan<<<1, 1024, 0, s>>>(blk_bytes, off, d.nblocks);
-    k_text_write<<<d.nblocks, kTextThreads, 0, s>>>(d, off, out);
+    k_text_write<<<d.nblocks, kTextThreads, 0, s>>>(d, unit_len, off, out);
     return 3;
 }
 

@@ -43,6 +43,7 @@ TextWriter::~TextWriter() {
     for (Slot& s : slot_) {
         cudaFree(s.text);
         cudaFree(s.blk);
+        cudaFree(s.unit_len);
         cudaFree(s.off);
         if (s.done) cudaEventDestroy(s.done);
     }
@@ -89,15 +90,18 @@ int TextWriter::submit(TextDoc& doc, cudaStream_t stream, const std::string& pat
     }
     if (s.blk_cap < nblocks) {
         cudaFree(s.blk);
+        cudaFree(s.unit_len);
         cudaFree(s.off);
         s.blk = nullptr;
+        s.unit_len = nullptr;
         s.off = nullptr;
         s.blk_cap = 0;
         TW_CUDA(cudaMalloc(&s.blk, (size_t)nblocks * sizeof(uint32_t)), "cudaMalloc(text blocks)");
-        TW_CUDA(cudaMalloc(&s.off, ((size_t)nblocks + 1) * sizeof(unsigned long long)), "cudaMalloc(text offsets)");
+        TW_CUDA(cudaMalloc(&s.unit_len, (size_t)nblocks * kTextBlockUnits * sizeof(uint16_t)), "cudaMalloc(text lengths)");
+        TW_CUDA(cudaMalloc(&s.off, ((size_t)nblocks + 2) * sizeof(unsigned long long)), "cudaMalloc(text offsets)");
         s.blk_cap = nblocks;
     }
-    const int nl = launch_text(doc, s.blk, s.off, s.text, stream);
+    const int nl = launch_text(doc, s.unit_len, s.blk, s.off, s.text, stream);
     if (launches) *launches = nl;
     TW_CUDA(cudaGetLastError(), "text kernels");
     TW_CUDA(cudaEventRecord(s.done, stream), "cudaEventRecord");
@@ -124,7 +128,7 @@ int TextWriter::wait(std::string* err) {
 void TextWriter::run() {
     cudaSetDevice(device_);
     bool ready = cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking) == cudaSuccess &&
-                 cudaHostAlloc(&total_, sizeof(unsigned long long), cudaHostAllocDefault) == cudaSuccess;
+                 cudaHostAlloc(&total_, 2 * sizeof(unsigned long long), cudaHostAllocDefault) == cudaSuccess;
     for (;;) {
         Job job;
         {
@@ -140,17 +144,17 @@ void TextWriter::run() {
         if (!ready) fail(MPH_ERR_CUDA, "text writer: stream set-up failed");
         // the document's bytes: count, then the text itself
         if (ok && (cudaStreamWaitEvent(copy_, s.done, 0) != cudaSuccess ||
-                   cudaMemcpyAsync(total_, s.off + job.nblocks, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                   copy_) != cudaSuccess ||
+                   cudaMemcpyAsync(total_, s.off + job.nblocks, 2 * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, copy_) != cudaSuccess ||
                    cudaStreamSynchronize(copy_) != cudaSuccess)) {
             ok = false;
             fail(MPH_ERR_CUDA, std::string("text writer: ") + cudaGetErrorString(cudaGetLastError()));
         }
         if (ok) {
-            bytes = (size_t)*total_;
-            if (bytes > s.cap) {
+            bytes = (size_t)total_[0];
+            if (bytes > s.cap || total_[1] != 0) {
                 ok = false;
-                fail(MPH_ERR_DEVICE, "text writer: document larger than its bound");
+                fail(MPH_ERR_DEVICE, "text writer: a record's text did not have its counted length");
             }
         }
         if (ok && bytes > pinned_cap_) {

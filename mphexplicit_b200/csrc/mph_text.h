@@ -30,6 +30,7 @@ enum TextRecord : int {
 // characters, of a float 13; "%d" at most 11).
 constexpr int kTextMaxRecord[kRecKinds] = {0, 103, 42, 14, 15, 12, 14, 2};
 constexpr int kTextMaxUnit = 256;     // a header or a record
+constexpr int kTextBlockUnits = 256;  // units (a header or a record) per block of the text kernels
 constexpr int kTextMaxSections = 12;
 constexpr int kTextHeadPool = 1536;
 constexpr int kTextValueStride = 16;  // mph_format_e: a length byte + at most 15 characters
@@ -60,7 +61,10 @@ int text_blocks(TextDoc& d);                 // assigns blocks; returns the grid
 size_t text_max_bytes(const TextDoc& d);     // an upper bound of the document's bytes
 // Three launches on s: per-block byte counts, their scan (off[nblocks] = total
 // bytes), the formatted text into out.  Returns the number of launches.
-int launch_text(const TextDoc& d, uint32_t* blk_bytes, unsigned long long* off, char* out, cudaStream_t s);
+// off has nblocks + 2 entries: off[nblocks + 1] != 0 flags a record whose text
+// did not have the length counted for it.
+int launch_text(const TextDoc& d, uint16_t* unit_len, uint32_t* blk_bytes, unsigned long long* off, char* out,
+                cudaStream_t s);
 void launch_text_values(const double* v, long long n, int as_float, char* out, cudaStream_t s);
 
 // Formats documents on the caller's stream and writes them to files from a
@@ -86,6 +90,7 @@ class TextWriter {
         char* text = nullptr;
         size_t cap = 0;
         uint32_t* blk = nullptr;
+        uint16_t* unit_len = nullptr;
         unsigned long long* off = nullptr;
         int blk_cap = 0;
         cudaEvent_t done = nullptr;
@@ -105,7 +110,7 @@ class TextWriter {
     cudaStream_t copy_ = nullptr;
     char* pinned_ = nullptr;
     size_t pinned_cap_ = 0;
-    unsigned long long* total_ = nullptr;  // pinned
+    unsigned long long* total_ = nullptr;  // pinned: {bytes, length-mismatch flag}
     std::mutex mu_;
     std::condition_variable cv_;
     std::deque<Job> q_;
