@@ -365,17 +365,36 @@ __global__ void __launch_bounds__(kTextThreads) k_text_count(const __grid_consta
 }
 
 // One block: exclusive scan of the block byte counts; total in off[nblocks].
+// Each thread takes 16 consecutive counts (four 16-byte loads) per pass.
 __global__ void __launch_bounds__(1024) k_text_scan(const uint32_t* __restrict__ blk_bytes,
                                                     unsigned long long* __restrict__ off, int nblocks) {
+    constexpr int kPer = 16;
     __shared__ unsigned long long ws[32];
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < nblocks; base += 1024) {
-        const int i = base + threadIdx.x;
-        const unsigned long long v = i < nblocks ? blk_bytes[i] : 0ull;
-        unsigned long long x = v;
+    for (int base = 0; base < nblocks; base += 1024 * kPer) {
+        const int i0 = base + threadIdx.x * kPer;
+        uint32_t v[kPer];
+        if (i0 + kPer <= nblocks) {
+            const uint4* p = reinterpret_cast<const uint4*>(blk_bytes + i0);  // i0 is a multiple of 16
+#pragma unroll
+            for (int q = 0; q < kPer / 4; ++q) {
+                const uint4 t = p[q];
+                v[4 * q] = t.x;
+                v[4 * q + 1] = t.y;
+                v[4 * q + 2] = t.z;
+                v[4 * q + 3] = t.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) v[q] = i0 + q < nblocks ? blk_bytes[i0 + q] : 0u;
+        }
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) sum += v[q];
+        unsigned long long x = sum;
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
@@ -392,7 +411,12 @@ __global__ void __launch_bounds__(1024) k_text_scan(const uint32_t* __restrict__
         }
         __syncthreads();
         const unsigned long long incl = x + (w ? ws[w - 1] : 0ull) + carry;
-        if (i < nblocks) off[i] = incl - v;
+        unsigned long long run = incl - sum;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            if (i0 + q < nblocks) off[i0 + q] = run;
+            run += v[q];
+        }
         __syncthreads();
         if (threadIdx.x == 1023) carry = incl;
         __syncthreads();

@@ -163,3 +163,47 @@ def test_text_buffers_reused():
         assert open(os.path.join(td, "a.vtk"), "rb").read() == open(os.path.join(td, "c.vtk"), "rb").read()
     assert M.format_e([]) == b""
     s.close()
+
+
+def test_cli_output_schedule_writes_behind_the_step():
+    """The drop-in executable (same arguments as MphExplicit) writes its *.prof
+    and *.vtk files behind the step; every file equals the host writers' bytes
+    on the FP64 state of that step, on the reference's schedule
+    (main.cpp:374-452)."""
+    import re
+    import subprocess
+    from tests.common import GoldenCase
+    case = GoldenCase("square_drop_skip")
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "mphexplicit_b200", "bin",
+                       "mph_b200")
+    with tempfile.TemporaryDirectory() as td:
+        text = open(case.data).read()
+        for key, val in (("OutputInterval", "1.0e-2"), ("VtkOutputInterval", "5.0e-3"), ("EndTime", "3.0e-2")):
+            text = re.sub(r"^%s\s+\S+" % key, "%s %s" % (key, val), text, flags=re.M)
+        data = os.path.join(td, "case.data")
+        open(data, "w").write(text)
+        r = subprocess.run([exe, data, case.grid, "p%03d.prof", "v%03d.vtk", "run.log", "1", "--dim=%d" % case.dim],
+                           cwd=td, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        p = M.read_data_file(data)
+        g = M.read_grid_file(case.grid)
+        s = M.Solver(p, g.header, g.type, g.xyz, g.vel, dim=case.dim)
+        t, dt, out_next, vtk_next, istep = g.header.time, p.dt, 0.0, 0.0, int(g.header.time / p.dt)
+        checked = 0
+        while t < p.end_time + 1.0e-5 * dt:
+            if t + 1.0e-5 * dt >= out_next:
+                _, hp = _host_bytes(s, td, t)
+                assert open(os.path.join(td, "p%03d.prof" % istep), "rb").read() == hp, istep
+                out_next += p.output_interval
+                checked += 1
+            s.step(1)
+            if t + 1.0e-5 * dt >= vtk_next:
+                s.compute_virial()
+                hv, _ = _host_bytes(s, td, t)
+                assert open(os.path.join(td, "v%03d.vtk" % istep), "rb").read() == hv, istep
+                vtk_next += p.vtk_output_interval
+                checked += 1
+            t += dt
+            istep += 1
+        assert checked >= 9
+        s.close()
