@@ -49,6 +49,24 @@ def dist_env():
         os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """x of the slowest rank: an all-reduce MAX over the process group (on the
+    GPU under NCCL, on the host under gloo)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(units_per_rank: int, steps: int, world: int, ms: float) -> float:
+    """Whole-job throughput: the units every rank updated over the slowest
+    rank's time (weak scaling: each rank runs its own replica)."""
+    return units_per_rank * steps * world / (ms / 1e3)
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -521,16 +539,13 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
     prof = s.profile_read()
     s.profile(False)
     info1 = s.info()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world)
     st = s.state()  # after warm + steps, for the cross-form error
     order = np.argsort(st["particle_index"], kind="stable")
     vel = st["vel"][order]
     fluid = st["type"][order] < 2
     n_fluid, n_all = sc.n_fluid, sc.n
-    out = {"mode": mode, "ms": ms, "value": n_fluid * args.steps * world / (ms / 1e3), "launches": launches,
+    out = {"mode": mode, "ms": ms, "value": job_value(n_fluid, args.steps, world, ms), "launches": launches,
            "prof": prof, "clocks": clk.summary(), "rebuilds": info1["rebuild_count"] - info0["rebuild_count"],
            "vel": vel, "fluid": fluid}
     # roofline of the dominant kernel: algorithmic bytes per particle the
@@ -564,11 +579,8 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
         ev1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3)
-        if world > 1:
-            t = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        out["e2e"] = {"value": n_fluid * ke * world / (e2e_ms / 1e3), "unit": UNIT,
+        e2e_ms = max_over_ranks(e2e_ms, world)
+        out["e2e"] = {"value": job_value(n_fluid, ke, world, e2e_ms), "unit": UNIT,
                       "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes),
                       "d2h_bytes_per_step": int(hx.nbytes + hv.nbytes), "steps": ke, "mode": mode}
     s.close()
