@@ -525,10 +525,10 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
     ev1 = torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
+    info0 = s.info()  # before the profiled window: it may compute output-only fields
     torch.cuda.synchronize()
     s.profile(True)
     l0 = s.launch_count()
-    info0 = s.info()
     with ClockSampler(gpu_index) as clk:
         ev0.record(stream)
         s.step(args.steps)

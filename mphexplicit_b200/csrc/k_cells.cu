@@ -145,11 +145,16 @@ __global__ void k_reorder(int n, const int* __restrict__ vals, const int* __rest
 // Neighbour list, one thread per particle (main.cpp:1329-1585).  The count and
 // the fill of the reference are one pass here: entries go to a column-major
 // [cap][n] table; a list longer than cap is still counted, raises
-// DEVFLAG_NEIGHBOR_OVERFLOW and the host rebuilds with a larger table.
+// DEVFLAG_NEIGHBOR_OVERFLOW and the host rebuilds with a larger table.  With
+// nlist_s, the entries within rs2 also go, in the same order, to the short
+// sublist: a particle moves at most MARGIN/2 between builds (the rebuild test
+// of main.cpp:1086-1108), so every pair within RadiusP until the next build is
+// in it, and a sum over the pairs within RadiusP visits them in list order.
 __global__ void __launch_bounds__(256)
 k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restrict__ keys,
                 const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist,
-                int cap, StepScalars* __restrict__ scal) {
+                int cap, int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s,
+                StepScalars* __restrict__ scal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const int ci = keys[i];
@@ -175,7 +180,8 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
     const double4 pi = pos[i];
     const int wall_begin = cellstart[c.tot], wall_end = cellstart[2 * c.tot];
     const size_t n = (size_t)c.n;
-    int cnt = 0;
+    int cnt = 0, cnt_s = 0;
+    const bool short_list = nlist_s != nullptr;
     for (int kind = 0; kind < 2; ++kind) {
         if (kind == 1 && wall_begin <= i && i < wall_end && cnt == 0) break;  // main.cpp:1416
         const int off = kind ? c.tot : 0;
@@ -190,6 +196,10 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
                 if (r2 <= c.rm2) {
                     if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
                     cnt++;
+                    if (short_list && r2 <= c.rs2) {
+                        if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
+                        cnt_s++;
+                    }
                 }
             }
         }
@@ -197,6 +207,11 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
     ncount[i] = cnt;
     atomicMax(&scal->max_neighbors, cnt);
     if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+    if (short_list) {
+        ncount_s[i] = cnt_s;
+        atomicMax(&scal->max_short, cnt_s);
+        if (cnt_s > cap_s) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+    }
 }
 
 __global__ void k_pack3(int n, const double4* __restrict__ src, double* __restrict__ dst) {
@@ -265,8 +280,10 @@ void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, cons
 }
 
 void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys, const int* cellstart,
-                          int* ncount, int* nlist, int cap, StepScalars* scal, cudaStream_t s) {
-    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, keys, cellstart, ncount, nlist, cap, scal);
+                          int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
+                          StepScalars* scal, cudaStream_t s) {
+    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, keys, cellstart, ncount, nlist, cap, ncount_s,
+                                                     nlist_s, cap_s, scal);
 }
 
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s) {

@@ -143,7 +143,12 @@ __device__ __forceinline__ double s_dwv(const SimConst& c, double q) { return c.
 // calculatePhysicalCoefficients (1631-1662) and the PressureP / PressureA
 // values (1904-1906, 1735-1740).  Every division of the reference is an
 // exactly rounded div_rn (mph_exact.cuh) against one reciprocal per pair.
-template <bool ST, bool RATIO>
+// DA: DensityA and PressureA are computed here, over the whole list.  Without
+// surface tension the step does not use them (PressureA is zero and its force
+// terms are not evaluated), so the step leaves them to k_density_a, run only
+// when they are read, and visits only the short sublist (the pairs that can
+// lie within RadiusP, in list order).
+template <bool ST, bool RATIO, bool DA>
 __global__ void __launch_bounds__(128, MPH_SWEEP_MINB)
 k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
           const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
@@ -175,7 +180,7 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-        const bool in_a = c.ra2 - r2 >= 0;
+        const bool in_a = DA && (c.ra2 - r2 >= 0);
         const bool in_p = c.rp2 - r2 >= 0;
         const bool in_g = ST && (c.rg2 - r2 >= 0);
         if (!(in_a || in_p || in_g)) continue;
@@ -207,7 +212,7 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
             sum_d -= u2 * e2 * dw;
         }
     }
-    dens_a[i] = sum_a;
+    if (DA) dens_a[i] = sum_a;
     const double strain = sum_p - c.n0p;
     strain_p[i] = strain;
     div_p[i] = sum_d;
@@ -215,11 +220,48 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
     if (strain < 0.0) kappa = 0.0;
     const double lambda = c.bulk_viscosity[ti];
     const double pp = -lambda * sum_d + kappa * strain;
-    double pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
-    if (c.n0a <= sum_a) pa = 0.0;
+    double pa = 0.0;
+    if (DA) {
+        pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
+        if (c.n0a <= sum_a) pa = 0.0;
+    }
     // sweep B gathers {v, PressureP} and {GravityCenter, PressureA} per neighbour
     velp[i] = make_double4(vi.x, vi.y, vi.z, pp);
     gcpa[i] = make_double4(g0, g1, g2, pa);
+}
+
+// DensityA (main.cpp:1665-1692) and PressureA (1735-1740) alone, for the
+// readers of a form without surface tension: the pairs of k_sweep_a's DensityA
+// sum in the same list order with the same arithmetic, from the positions
+// that sweep used (the step changes only velocities after it), so the values
+// are those the reference holds after the step.
+template <bool RATIO>
+__global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __restrict__ pos,
+                                                   const int* __restrict__ ncount, const int* __restrict__ nlist,
+                                                   double* __restrict__ dens_a, double4* __restrict__ gcpa) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const double4 pi = pos[i];
+    const int ti = type_of(pi);
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    double sum_a = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+        const int j = __ldg(nlist + (size_t)k * n + i);
+        if (j == i) continue;
+        const double4 pj = pos[j];
+        double x[3];
+        disp(c, pi, pj, x);
+        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(c.ra2 - r2 >= 0)) continue;
+        const double r = sqrt(r2);
+        const double qa = div_rn(r, c.ra, c.inv_ra);
+        sum_a += RATIO ? c.ratio[ti][type_of(pj)] * s_wa(c, qa) : s_wa(c, qa);
+    }
+    dens_a[i] = sum_a;
+    double pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
+    if (c.n0a <= sum_a) pa = 0.0;
+    reinterpret_cast<double*>(gcpa + i)[3] = pa;
 }
 
 // Sweep B: PressureP force (main.cpp:1908-1938), PressureA force
@@ -706,22 +748,29 @@ void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4*
 }
 
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,
-                    const int* ncount, const int* nlist, int cap_stride, double* dens_a, double* strain_p,
-                    double* div_p, double4* press, double4* gc, double* wall_center, cudaStream_t s) {
+                    const int* ncount, const int* nlist, const int* ncount_s, const int* nlist_s, double* dens_a,
+                    double* strain_p, double* div_p, double4* press, double4* gc, double* wall_center,
+                    cudaStream_t s) {
     (void)cellstart;
-    (void)cap_stride;
     const int nb = blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1;
+#define SWEEP_A(ST, RATIO, CNT, LIST)                                                                             \
+    k_sweep_a<ST, RATIO, ST><<<nb, 128, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p, div_p, press, gc, \
+                                                wall_center)
     if (c.has_st) {
-        if (c.ratio_all_one)
-            k_sweep_a<true, false><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
-        else
-            k_sweep_a<true, true><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+        if (c.ratio_all_one) SWEEP_A(true, false, ncount, nlist); else SWEEP_A(true, true, ncount, nlist);
     } else {
-        if (c.ratio_all_one)
-            k_sweep_a<false, false><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
-        else
-            k_sweep_a<false, true><<<nb, 128, 0, s>>>(c, pos, vel, ncount, nlist, dens_a, strain_p, div_p, press, gc, wall_center);
+        if (c.ratio_all_one) SWEEP_A(false, false, ncount_s, nlist_s); else SWEEP_A(false, true, ncount_s, nlist_s);
     }
+#undef SWEEP_A
+}
+
+void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, const int* nlist, double* dens_a,
+                      double4* gc, cudaStream_t s) {
+    const int nb = blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1;
+    if (c.ratio_all_one)
+        k_density_a<false><<<nb, 128, 0, s>>>(c, pos, ncount, nlist, dens_a, gc);
+    else
+        k_density_a<true><<<nb, 128, 0, s>>>(c, pos, ncount, nlist, dens_a, gc);
 }
 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,

@@ -80,6 +80,7 @@ struct mph_ctx {
     double time = 0.0;
     long long step = 0, rebuilds = 0;
     bool virial_valid = false;
+    bool dens_a_valid = false;  // DensityA / PressureA hold the values of the last step
     int max_neighbors = 0;
     long long launches = 0;
     Profiler prof;
@@ -272,6 +273,8 @@ int mph::make_simconst(const mph_params& p, const mph_grid_header& h, const mph_
         { msg = "too many cells"; return MPH_ERR_GEOMETRY; }
     const double rm = c.max_radius + 0.1 * l0;  // MaxRadius + MARGIN
     s.rm2 = rm * rm;
+    const double rs = (c.radius_p + 0.1 * l0) * (1.0 + 1e-9);  // RadiusP + MARGIN, with room for rounding
+    s.rs2 = rs * rs;
     s.range[0] = (int)std::ceil(rm / c.cell_width[0]);
     s.range[1] = (int)std::ceil(rm / c.cell_width[1]);
     s.range[2] = dim == 2 ? 0 : (int)std::ceil(rm / c.cell_width[2]);
@@ -356,7 +359,8 @@ static int dalloc(mph_ctx* ctx, T** ptr, size_t count) {
 static void free_fp64(mph::DevFP64& d) {
     void* ptrs[] = {d.pidx[0], d.pidx[1], d.type[0], d.type[1], d.pos[0], d.pos[1], d.vel[0], d.vel[1],
                     d.snap, d.force, d.dens_a, d.strain_p, d.div_p, d.press, d.gc, d.virial_p, d.keys,
-                    d.vals, d.cellstart, d.ncount, d.nlist, d.wall_center, d.staging, d.scal};
+                    d.vals, d.cellstart, d.ncount, d.nlist, d.ncount_s, d.nlist_s, d.wall_center, d.staging,
+                    d.scal};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     d = mph::DevFP64();
@@ -401,8 +405,8 @@ static int alloc_fp64(mph_ctx* ctx) {
 
 // Initial list length: lattice points within the cut-off, with head room for
 // compression; the build grows it when a longer list appears.
-static int initial_capacity(const mph_ctx* ctx) {
-    const double ratio = std::sqrt(ctx->sc.rm2) / ctx->h.particle_spacing;
+static int initial_capacity(const mph_ctx* ctx, double r2) {
+    const double ratio = std::sqrt(r2) / ctx->h.particle_spacing;
     const int r = (int)ratio + 1;
     int cnt = 0;
     const int zr = ctx->dim == 2 ? 0 : r;
@@ -415,17 +419,21 @@ static int initial_capacity(const mph_ctx* ctx) {
     return cap;
 }
 
-static int grow_list(mph_ctx* ctx, int need) {
-    mph::DevFP64& d = ctx->d;
+static int grow_table(mph_ctx* ctx, int need, int** table, int* capacity) {
     int cap = (int)(need * 1.15) + 8;
     cap = (cap + 31) / 32 * 32;
-    if (d.nlist) cudaFree(d.nlist);
-    d.nlist = nullptr;
-    d.cap = 0;
-    TRY(dalloc(ctx, &d.nlist, (size_t)cap * (size_t)ctx->n));
-    d.cap = cap;
+    if (*table) cudaFree(*table);
+    *table = nullptr;
+    *capacity = 0;
+    TRY(dalloc(ctx, table, (size_t)cap * (size_t)ctx->n));
+    *capacity = cap;
     return MPH_OK;
 }
+
+static int grow_list(mph_ctx* ctx, int need) { return grow_table(ctx, need, &ctx->d.nlist, &ctx->d.cap); }
+
+// The short sublist serves sweep A when there is no surface tension.
+static bool uses_short_list(const mph_ctx* ctx) { return !ctx->sc.has_st; }
 
 // calculateCellParticle + calculateNeighbor (main.cpp:1111-1596).
 static int rebuild_fp64(mph_ctx* ctx) {
@@ -443,20 +451,27 @@ static int rebuild_fp64(mph_ctx* ctx) {
     }
     d.cur = b;
     d.vcur = vb;
+    const bool sl = uses_short_list(ctx);
+    int max_short = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
         CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), st));
+        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_short, 0, sizeof(int), st));
         {
             Launch L(ctx, "neighbor_list");
-            mph::launch_neighbor_list(s, d.pos[d.cur], d.keys, d.cellstart, d.ncount, d.nlist, d.cap, d.scal, st);
+            mph::launch_neighbor_list(s, d.pos[d.cur], d.keys, d.cellstart, d.ncount, d.nlist, d.cap,
+                                      sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.cap_s, d.scal, st);
         }
         CUDA_TRY(ctx, cudaGetLastError());
         CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scal, d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(ctx, cudaStreamSynchronize(st));
         ctx->max_neighbors = ctx->h_scal->max_neighbors;
-        if (ctx->h_scal->max_neighbors <= d.cap) break;
-        TRY(grow_list(ctx, ctx->h_scal->max_neighbors));
+        max_short = sl ? ctx->h_scal->max_short : 0;
+        if (ctx->max_neighbors <= d.cap && max_short <= d.cap_s) break;
+        if (ctx->max_neighbors > d.cap) TRY(grow_list(ctx, ctx->max_neighbors));
+        if (max_short > d.cap_s) TRY(grow_table(ctx, max_short, &d.nlist_s, &d.cap_s));
     }
-    if (ctx->max_neighbors > d.cap) return fail(ctx, MPH_ERR_CAPACITY, "neighbour table could not grow");
+    if (ctx->max_neighbors > d.cap || max_short > d.cap_s)
+        return fail(ctx, MPH_ERR_CAPACITY, "neighbour table could not grow");
     // the overflow flag of the attempts that grew the table is not an error
     CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->flags, 0, sizeof(int), st));
     ctx->lrn.edges_valid = false;
@@ -466,8 +481,20 @@ static int rebuild_fp64(mph_ctx* ctx) {
 static void sweep_a(mph_ctx* ctx, bool advance_wall) {
     mph::DevFP64& d = ctx->d;
     Launch L(ctx, "sweep_a");
-    mph::launch_sweep_a(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.ncount, d.nlist, d.cap, d.dens_a,
-                        d.strain_p, d.div_p, d.press, d.gc, advance_wall ? d.wall_center : nullptr, ctx->stream);
+    mph::launch_sweep_a(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.ncount, d.nlist, d.ncount_s, d.nlist_s,
+                        d.dens_a, d.strain_p, d.div_p, d.press, d.gc, advance_wall ? d.wall_center : nullptr,
+                        ctx->stream);
+    ctx->dens_a_valid = ctx->sc.has_st;  // without surface tension, computed when read
+}
+
+// DensityA / PressureA of the last step, for a reader (FP64 and learned forms
+// without surface tension, where the step itself does not need them).
+static void ensure_density_a(mph_ctx* ctx) {
+    if (ctx->mixed || ctx->dens_a_valid) return;
+    mph::DevFP64& d = ctx->d;
+    Launch L(ctx, "density_a");
+    mph::launch_density_a(ctx->sc, d.pos[d.cur], d.ncount, d.nlist, d.dens_a, d.gc, ctx->stream);
+    ctx->dens_a_valid = true;
 }
 
 static int validate_inputs(int n, const int* type, const double* xyz, const double* vel) {
@@ -533,7 +560,11 @@ static int create_impl(mph_ctx* ctx, const int* type, const double* xyz, const d
     if (ctx->mode == MPH_MODE_MIXED || ctx->mode == MPH_MODE_MIXED_P64) {
         TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, ctx->mode == MPH_MODE_MIXED_P64, st, &ctx->err));
     } else {
-        TRY(grow_list(ctx, initial_capacity(ctx)));
+        TRY(grow_list(ctx, initial_capacity(ctx, ctx->sc.rm2)));
+        if (uses_short_list(ctx)) {
+            TRY(dalloc(ctx, &d.ncount_s, n));
+            TRY(grow_table(ctx, initial_capacity(ctx, ctx->sc.rs2), &d.nlist_s, &d.cap_s));
+        }
         TRY(rebuild_fp64(ctx));
         sweep_a(ctx, false);
     }
@@ -875,6 +906,7 @@ extern "C" int mph_synchronize(mph_ctx* ctx) {
 // The mixed form keeps its own particle order between rebuilds; bring the
 // FP64 buffers up to date before any read-back.
 static int sync_state(mph_ctx* ctx) {
+    ensure_density_a(ctx);
     if (ctx->mixed) {
         Launch L(ctx, "mix_export");
         const int rc = mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err, &L.count);
@@ -955,6 +987,7 @@ extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, doubl
 
 extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    ensure_density_a(ctx);  // from the positions the last step used, before they are replaced
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     cudaStream_t st = ctx->stream;
@@ -1038,6 +1071,7 @@ extern "C" int mph_compute_virial(mph_ctx* ctx) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
     if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "virial stress is computed by the FP64 form");
     mph::DevFP64& d = ctx->d;
+    ensure_density_a(ctx);  // the virial reads PressureA
     {
         Launch L(ctx, "virial");
         mph::launch_virial(ctx->sc, d.pos[d.cur], d.vel[d.vcur], d.press, d.gc, d.ncount, d.nlist, d.virial_p,

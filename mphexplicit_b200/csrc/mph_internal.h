@@ -30,6 +30,7 @@ struct SimConst {
     double ra, rg, rp, rv;             // radii
     double ra2, rg2, rp2, rv2;         // radius*radius
     double rm2;                        // (MaxRadius+MARGIN)^2, neighbour cut-off
+    double rs2;                        // ((RadiusP+MARGIN)(1+1e-9))^2, cut-off of the short sublist
     double ca, cg, cp, cv;             // (1/Sw)/h^D for wa, wg/dwg, wp/dwp, dwv
     double inv_ra, inv_rg, inv_rp, inv_rv;  // 1.0/h
     double m2_rg, m2_rp, m2_rv;        // -2.0/h
@@ -86,6 +87,9 @@ struct DevFP64 {
     int* ncount = nullptr;                  // NeighborCount
     int* nlist = nullptr;                   // [cap][n] column-major list
     int cap = 0;
+    int* ncount_s = nullptr;                // short sublist (no surface tension): the entries
+    int* nlist_s = nullptr;                 // within rs2, in list order, [cap_s][n]
+    int cap_s = 0;
     double* wall_center = nullptr;          // [4][3], advanced on the device
     double* staging = nullptr;              // [n][3] pack/unpack buffer
     StepScalars* scal = nullptr;
@@ -99,9 +103,11 @@ void launch_cell_ranges(const SimConst& c, const int* keys, int* cellstart, cuda
 void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, const int* type_in,
                     const double4* pos_in, const double4* vel_in, int* pidx_out, int* type_out,
                     double4* pos_out, double4* vel_out, double4* snap, cudaStream_t s);
+// nlist_s != nullptr: also the short sublist (entries within rs2, in list
+// order; its longest length in scal->max_short).
 void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys,
                           const int* cellstart, int* ncount, int* nlist, int cap,
-                          StepScalars* scal, cudaStream_t s);
+                          int* ncount_s, int* nlist_s, int cap_s, StepScalars* scal, cudaStream_t s);
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);
 void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s);
 
@@ -109,10 +115,16 @@ void launch_unpack3(int n, const double* src, double4* dst, const int* type, cud
 void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel,
                  const double4* snap, const double* wall_center, StepScalars* scal,
                  cudaStream_t s);
+// Without surface tension sweep A visits the short sublist (ncount_s,
+// nlist_s); with it, the whole list.
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
-                    const double4* vel, const int* ncount, const int* nlist, int cap_stride,
-                    double* dens_a, double* strain_p, double* div_p, double4* press, double4* gc,
-                    double* wall_center, cudaStream_t s);
+                    const double4* vel, const int* ncount, const int* nlist, const int* ncount_s,
+                    const int* nlist_s, double* dens_a, double* strain_p, double* div_p, double4* press,
+                    double4* gc, double* wall_center, cudaStream_t s);
+// DensityA and PressureA alone (into dens_a and gc[].w), in k_sweep_a's
+// order: what sweep A leaves out when there is no surface tension.
+void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, const int* nlist, double* dens_a,
+                      double4* gc, cudaStream_t s);
 // eforce != nullptr: the learned form (edge-MLP pair forces replace the
 // PressureA, DiffuseInterface and ViscosityV terms; see k_sweep_b)
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
