@@ -278,11 +278,19 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
           const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
           const int* __restrict__ ncount, const int* __restrict__ nlist, double4* __restrict__ force,
           StepScalars* __restrict__ scal, const int* __restrict__ eoff, const float4* __restrict__ eforce,
-          float4* __restrict__ lsum) {
+          float4* __restrict__ lsum, int part) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
-    const double4 pi = pos[i];
+    const int nf = cellstart[c.tot];
     const double4 vi = velp[i];   // .w = PressureP
+    // part 1: fluid only; a wall keeps its velocity (what the full sweep
+    // writes for it) and its force is left for part 2 (output only)
+    if (part == 1 && i >= nf) {
+        vel_out[i] = make_double4(vi.x, vi.y, vi.z, 0.0);
+        return;
+    }
+    if (part == 2 && i < nf) return;
+    const double4 pi = pos[i];
     const int ti = type_of(pi);
     const double ai = c.a_k[ti];
     double4 gci = make_double4(0, 0, 0, 0);
@@ -371,7 +379,6 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
             fv2 += div_rn(cm * dot * e2 * dw, r, ri) * c.vol;
         }
     }
-    const int nf = cellstart[c.tot];
     if (LRN) {
         float l0 = 0.f, l1 = 0.f, l2 = 0.f;
         if (i < nf) {
@@ -404,7 +411,7 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         if (!(isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
     }
     force[i] = make_double4(F0, F1, F2, 0.0);
-    vel_out[i] = vn;
+    if (part != 2) vel_out[i] = vn;
 }
 
 // Self-check of div_rn against the hardware IEEE division: operands with
@@ -776,12 +783,12 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
                     double4* vel_out, const double4* press, const double4* gc, const int* ncount,
                     const int* nlist, double4* force, StepScalars* scal, cudaStream_t s, const int* eoff,
-                    const float4* eforce, float4* lsum) {
+                    const float4* eforce, float4* lsum, int part) {
     (void)vel_in;
     const int nb = blocks(c.n, 128);
 #define SWEEP_B(ST, RATIO, LRN) \
     k_sweep_b<ST, RATIO, LRN><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal, \
-                                                 eoff, eforce, lsum)
+                                                 eoff, eforce, lsum, part)
 #define SWEEP_B2(ST, RATIO) \
     if (eforce) SWEEP_B(ST, RATIO, true); else SWEEP_B(ST, RATIO, false)
     if (c.has_st) {

@@ -81,6 +81,7 @@ struct mph_ctx {
     long long step = 0, rebuilds = 0;
     bool virial_valid = false;
     bool dens_a_valid = false;  // DensityA / PressureA hold the values of the last step
+    bool wall_force_valid = true;  // the walls' Force holds the values of the last step
     int max_neighbors = 0;
     long long launches = 0;
     Profiler prof;
@@ -497,6 +498,17 @@ static void ensure_density_a(mph_ctx* ctx) {
     ctx->dens_a_valid = true;
 }
 
+// The walls' Force of the last step (output only: walls do not move by it),
+// from the arrays the step's force sweep read, which stay until the next step.
+static void ensure_wall_force(mph_ctx* ctx) {
+    if (ctx->mixed || ctx->wall_force_valid) return;
+    mph::DevFP64& d = ctx->d;
+    Launch L(ctx, "wall_force");
+    mph::launch_sweep_b(ctx->sc, d.cellstart, d.pos[d.cur], nullptr, nullptr, d.press, d.gc, d.ncount, d.nlist,
+                        d.force, d.scal, ctx->stream, nullptr, nullptr, nullptr, 2);
+    ctx->wall_force_valid = true;
+}
+
 static int validate_inputs(int n, const int* type, const double* xyz, const double* vel) {
     for (int i = 0; i < n; ++i) {
         if (type[i] < 0 || type[i] >= MPH_TYPE_COUNT) return fail(nullptr, MPH_ERR_ARG, "particle type outside 0..3");
@@ -642,7 +654,8 @@ static int step_fp64(mph_ctx* ctx, int nsteps) {
         {
             Launch L(ctx, "sweep_b");
             mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.vel[1 - d.vcur], d.press, d.gc,
-                                d.ncount, d.nlist, d.force, d.scal, st);
+                                d.ncount, d.nlist, d.force, d.scal, st, nullptr, nullptr, nullptr, 1);
+            ctx->wall_force_valid = false;  // computed when read
         }
         d.vcur = 1 - d.vcur;
         CUDA_TRY(ctx, cudaGetLastError());
@@ -803,8 +816,11 @@ static int step_learned(mph_ctx* ctx, int nsteps) {
             }
             {
                 Launch Lb(ctx, "sweep_b_learned");
-                mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vout, d.press, d.gc, d.ncount,
-                                    d.nlist, d.force, d.scal, st, L.eoff, L.eforce, L.lsum);
+                // the learned sweep evaluates only the pairs within RadiusP
+                const bool sl = uses_short_list(ctx);
+                mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vout, d.press, d.gc,
+                                    sl ? d.ncount_s : d.ncount, sl ? d.nlist_s : d.nlist, d.force, d.scal, st,
+                                    L.eoff, L.eforce, L.lsum);
             }
             bool use = true;
             if (L.info.steps % L.judge_interval == 0) {
@@ -907,6 +923,7 @@ extern "C" int mph_synchronize(mph_ctx* ctx) {
 // FP64 buffers up to date before any read-back.
 static int sync_state(mph_ctx* ctx) {
     ensure_density_a(ctx);
+    ensure_wall_force(ctx);
     if (ctx->mixed) {
         Launch L(ctx, "mix_export");
         const int rc = mph::mixed_export(ctx->mixed, ctx->sc, ctx->d, ctx->stream, &ctx->err, &L.count);
@@ -988,6 +1005,7 @@ extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, doubl
 extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
     ensure_density_a(ctx);  // from the positions the last step used, before they are replaced
+    ensure_wall_force(ctx);
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     cudaStream_t st = ctx->stream;

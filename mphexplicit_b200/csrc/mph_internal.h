@@ -126,12 +126,15 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
 void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, const int* nlist, double* dens_a,
                       double4* gc, cudaStream_t s);
 // eforce != nullptr: the learned form (edge-MLP pair forces replace the
-// PressureA, DiffuseInterface and ViscosityV terms; see k_sweep_b)
+// PressureA, DiffuseInterface and ViscosityV terms; see k_sweep_b; it then
+// needs only the pairs within RadiusP, so the short sublist may be passed).
+// part: 0 every particle; 1 the fluid (walls copy their velocity, their
+// force is not written); 2 the walls' forces alone (vel_out unused).
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel_in, double4* vel_out, const double4* press,
                     const double4* gc, const int* ncount, const int* nlist, double4* force,
                     StepScalars* scal, cudaStream_t s, const int* eoff = nullptr,
-                    const float4* eforce = nullptr, float4* lsum = nullptr);
+                    const float4* eforce = nullptr, float4* lsum = nullptr, int part = 0);
 
 // ---- learned form (k_fp64.cu) ---------------------------------------------
 // CSR edges of the fluid particles' lists (i < nf): eoff[0..nf] = exclusive
