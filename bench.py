@@ -76,12 +76,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_bf16_peak() -> float:
+def measured_bf16_peak():
+    """Dense BF16 peak (TFLOP/s) and where it comes from."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         with open(p) as f:
-            return float(json.load(f)["bf16_tflops"])
-    return 1590.0
+            return float(json.load(f)["bf16_tflops"]), "measured bf16 burst (MEASURED_PEAKS.json)"
+    return 1590.0, "fallback (MEASURED_PEAKS.json absent)"
 
 
 def ncu_traffic(kernel: str, mode: str):
@@ -237,11 +238,11 @@ def measure_learned(args, rank):
         nl, tot = prof["mlp_edges"]
         avg_s = tot / max(1, nl) / 1e3
         tflops = stats["edges"] * MLP_FLOPS_PER_EDGE / avg_s / 1e12
-        peak = measured_bf16_peak()
+        peak, peak_kind = measured_bf16_peak()
         out["roofline"] = {"kernel": "mlp_edges", "bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
                            "frac": tflops / peak, "edges_per_launch": stats["edges"],
                            "flops_per_edge": MLP_FLOPS_PER_EDGE, "avg_launch_ms": avg_s * 1e3,
-                           "peak_source": "measured bf16 burst (MEASURED_PEAKS.json)"}
+                           "peak_source": peak_kind}
     return out
 
 
