@@ -555,7 +555,7 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
     name, (nl, tot_ms) = max(prof.items(), key=lambda kv: kv[1][1])
     avg_s = tot_ms / args.steps / 1e3
     peak, peak_kind = measured_peaks()
-    units = n_fluid if name == "mix_sweep_b" else n_all
+    units = n_fluid if name in ("mix_sweep_b", "sweep_b") else n_all  # the force sweeps update the fluid
     algo = ALGO_BYTES.get(name, 0.0) * units
     achieved = algo / avg_s / 1e9
     out["roofline"] = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
