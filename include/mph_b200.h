@@ -181,7 +181,10 @@ int mph_get_constants(mph_ctx* ctx, mph_constants* c);
  * (cell-sorted) order, as the reference's arrays are after a step.  Any pointer
  * may be NULL.  particle_index[i] is the file-order id of slot i
  * (ParticleIndex, main.cpp:75).  virial_pressure is valid after
- * mph_compute_virial. */
+ * mph_compute_virial.  Values the step itself does not need (DensityA without
+ * surface tension, the walls' Force) are computed on the first read after a
+ * step, from the arrays that step used: the same values as computing them in
+ * the step, at the cost of a launch in this call. */
 int mph_get_state(mph_ctx* ctx, int* particle_index, int* type,
                   double* xyz, double* vel, double* force, int* neighbor_count,
                   double* density_a, double* vol_strain_p, double* virial_pressure);
