@@ -187,7 +187,6 @@ void TextWriter::run() {
                 const bool wrote = std::fwrite(pinned_, 1, bytes, fp) == bytes;
                 const bool closed = std::fclose(fp) == 0;
                 if (!wrote || !closed) fail(MPH_ERR_IO, "cannot write " + job.path);
-                else bytes_ += (long long)bytes;
             }
         }
         {

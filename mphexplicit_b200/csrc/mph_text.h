@@ -83,7 +83,6 @@ class TextWriter {
     // Waits for every submitted write; returns the first failure since the
     // last wait (MPH_OK if none) with its message in *err.
     int wait(std::string* err);
-    long long bytes_written() const { return bytes_; }
 
   private:
     struct Slot {
@@ -118,7 +117,6 @@ class TextWriter {
     bool stop_ = false;
     int err_code_ = 0;
     std::string err_msg_;
-    long long bytes_ = 0;
     std::thread th_;
 };
 
