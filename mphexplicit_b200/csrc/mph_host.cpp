@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <string>
 #include <vector>
 #include <algorithm>
@@ -1106,7 +1107,11 @@ static int text_submit(mph_ctx* ctx, mph::TextDoc& doc, const char* path, const 
     if (!ctx->text) {
         int dev = 0;
         CUDA_TRY(ctx, cudaGetDevice(&dev));
-        ctx->text = new mph::TextWriter(dev);
+        try {
+            ctx->text = new mph::TextWriter(dev);
+        } catch (const std::exception& e) {  // no exception crosses the C ABI
+            return fail(ctx, MPH_ERR_NOMEM, std::string("text writer thread: ") + e.what());
+        }
     }
     std::string err;
     Launch L(ctx, what);
