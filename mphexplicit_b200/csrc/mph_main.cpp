@@ -1,6 +1,6 @@
 // mph_main.cpp — command-line drop-in for the reference solver executable.
 //
-//   mph_b200 [data grid prof vtk log nthreads] [--dim=2|3] [--mode=fp64|mixed]
+//   mph_b200 [data grid prof vtk log nthreads] [--dim=2|3] [--mode=fp64|mixed|mixed_p64]
 //
 // Same positional arguments and defaults as the reference's main()
 // (main.cpp:293-307; nthreads is accepted and ignored: the step runs on the
@@ -32,10 +32,27 @@ static void log_printf(const char* fmt, ...) {
     va_end(b);
 }
 
-static int die(mph_ctx* ctx, int st, const char* what) {
-    char msg[512];
+static const char* status_text(int st) {
+    switch (st) {
+        case MPH_ERR_ARG: return "invalid argument";
+        case MPH_ERR_IO: return "file could not be opened or parsed";
+        case MPH_ERR_CUDA: return "CUDA runtime error";
+        case MPH_ERR_CAPACITY: return "a device capacity was exceeded";
+        case MPH_ERR_DEVICE: return "a device error flag was raised";
+        case MPH_ERR_NONFINITE: return "NaN or Inf in the particle state";
+        case MPH_ERR_STATE: return "call not valid in this state";
+        case MPH_ERR_NOMEM: return "allocation failed";
+        case MPH_ERR_GEOMETRY: return "cell grid incompatible with the radius";
+        default: return "error";
+    }
+}
+
+// Logs the failure (the library's message, else the status meaning) and ends.
+static int die(mph_ctx* ctx, int st, const char* what, const char* path = nullptr) {
+    char msg[512] = {0};
     mph_last_error(ctx, msg, sizeof(msg));
-    log_printf("error %d in %s: %s\n", st, what, msg);
+    log_printf("error %d in %s%s%s: %s\n", st, what, path ? " " : "", path ? path : "",
+               msg[0] ? msg : status_text(st));
     if (ctx) mph_destroy(ctx);
     if (g_log) std::fclose(g_log);
     return 1;
@@ -54,8 +71,13 @@ int main(int argc, char** argv) {
         const std::string a = argv[i];
         if (a.rfind("--dim=", 0) == 0) dim = std::atoi(a.c_str() + 6);
         else if (a == "--mode=mixed") mode = MPH_MODE_MIXED;
+        else if (a == "--mode=mixed_p64") mode = MPH_MODE_MIXED_P64;
         else if (a == "--mode=fp64") mode = MPH_MODE_FP64;
-        else pos.push_back(a);
+        else if (a.rfind("--", 0) == 0) {
+            std::fprintf(stderr, "unknown option %s\nusage: %s [data grid prof vtk log nthreads] [--dim=2|3] "
+                                 "[--mode=fp64|mixed|mixed_p64]\n", a.c_str(), argv[0]);
+            return 2;
+        } else pos.push_back(a);
     }
     if (pos.size() > 0) data = pos[0];
     if (pos.size() > 1) grid = pos[1];
@@ -72,15 +94,15 @@ int main(int argc, char** argv) {
     mph_params_defaults(&p);
     int bad = 0;
     int st = mph_read_data_file(data.c_str(), &p, &bad);
-    if (st != MPH_OK) return die(nullptr, st, "reading the data file");
+    if (st != MPH_OK) return die(nullptr, st, "reading the data file", data.c_str());
     if (bad) log_printf("%d invalid line(s) in data file \"%s\"\n", bad, data.c_str());
     mph_grid_header h;
     st = mph_read_grid_header(grid.c_str(), &h);
-    if (st != MPH_OK) return die(nullptr, st, "reading the grid header");
+    if (st != MPH_OK) return die(nullptr, st, "reading the grid header", grid.c_str());
     std::vector<int> type(h.particle_count);
     std::vector<double> x(3 * (size_t)h.particle_count), v(3 * (size_t)h.particle_count);
     st = mph_read_grid_file(grid.c_str(), &h, h.particle_count, type.data(), x.data(), v.data());
-    if (st != MPH_OK) return die(nullptr, st, "reading the grid file");
+    if (st != MPH_OK) return die(nullptr, st, "reading the grid file", grid.c_str());
     {
         time_t t = time(NULL);
         log_printf("start initialization at %s\n", ctime(&t));
