@@ -404,7 +404,7 @@ def measure_output(args, sc, rank):
     s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=3, mode="mixed_p64")
     s.step(20)
     s.synchronize()
-    out = {"workload": workload_name(sc), "particles": sc.n}
+    out = {"workload": scene_workload(sc), "particles": sc.n}
     with tempfile.TemporaryDirectory() as td:
         vtk, prof, host = (os.path.join(td, f) for f in ("d.vtk", "d.prof", "h.vtk"))
         s.write_vtk(vtk)  # warm-up: buffers, writer thread
@@ -455,56 +455,92 @@ def measure_output(args, sc, rank):
     return out
 
 
+SCENES = {  # bench scene -> dam-break fluid block and box (cells); 3 wall layers, l0 = 0.005 m
+    "dam": ((100, 100, 200), (300, 100, 240)),
+    "dam_mid": ((80, 80, 160), (240, 80, 192)),   # the 1 M-fluid scaled dam break (benchmark config 5)
+    "dam_small": ((40, 40, 80), (120, 40, 96)),
+}
+
+
 def make_scene(args, rank):
     from mphexplicit_b200 import scenes
-    if args.scene == "dam":
-        return scenes.dam_break_3d(seed=rank)
-    if args.scene == "dam_small":
-        return scenes.dam_break_3d(fluid=(40, 40, 80), box=(120, 40, 96), seed=rank)
-    if args.scene == "dam_mid":  # the 1 M-fluid scaled dam break (benchmark config 5)
-        return scenes.dam_break_3d(fluid=(80, 80, 160), box=(240, 80, 192), seed=rank)
-    raise SystemExit("unknown scene " + args.scene)
+    if args.scene not in SCENES:
+        raise SystemExit("unknown scene " + args.scene)
+    fluid, box = SCENES[args.scene]
+    return scenes.dam_break_3d(fluid=fluid, box=box, seed=rank)
 
 
-def workload_name(sc) -> str:
-    m = sc.meta
+def workload_name(fluid, box, walls, l0, n, n_fluid) -> str:
     return ("dam_break_3d fluid %dx%dx%d in a %dx%dx%d-cell box, %d wall layers, l0=%g: %d particles (%d fluid)"
-            % (*m["fluid"], *m["box"], m["walls"], m["l0"], sc.n, sc.n_fluid))
+            % (*fluid, *box, walls, l0, n, n_fluid))
 
 
-def cpu_baseline(sc, seconds_budget: float, steps: int):
-    """The reference's own step (oracle/_ref, OpenMP, all host threads) on the
-    same scene; a bounded sample: the steps that fit in the budget."""
-    from oracle import pyoracle as po
-    threads = os.cpu_count() or 1
+def scene_workload(sc) -> str:
+    m = sc.meta
+    return workload_name(m["fluid"], m["box"], m["walls"], m["l0"], sc.n, sc.n_fluid)
+
+
+def bench_config(workload: str, mode: str) -> dict:
+    """The `config` object, identical in the product's line and the reference
+    arm's line for the same workload and arithmetic."""
+    return {"workload": workload, "form": mode,
+            "arithmetic": "fp64 (the reference's)" if mode == "fp64" else "fp32 pairs + fp64 integration",
+            "l2": "inputs larger than L2 (particle state and neighbour lists, several GB)"}
+
+
+def cpu_reference_sample(args, threads: int, steps: int, warmup: int, budget: float, rebuild_at: int):
+    """The reference's own step (oracle/_ref/ref_mph3d, OpenMP) on the bench
+    scene, written by oracle/ref_inputs (nothing of the product is loaded):
+    `warmup` untimed steps, then up to `steps` timed steps (stopping after the
+    step that crosses `budget` seconds), the `rebuild_at`-th of which rebuilds
+    the cell and neighbour lists (the developed flow rebuilds about every 20
+    steps; a dam break at rest does not for its first few hundred)."""
+    from oracle import ref_inputs as RI
+    fluid, box = SCENES[args.scene]
     with tempfile.TemporaryDirectory() as td:
-        d, g = os.path.join(td, "b.data"), os.path.join(td, "b.grid")
-        sc.write(d, g)
-        if po.ref_available(sc.dim):
-            r = po.time_reference(d, g, sc.dim, 0, steps, threads, max_seconds=seconds_budget, timeout=1800)
-            kind = "reference"
-        else:
-            os.environ["OMP_NUM_THREADS"] = str(threads)
-            r = po.time_oracle(sc, 0, steps, max_seconds=seconds_budget)
-            kind = "port"
-    val = r["fluid"] * r["steps"] / r["seconds"]
-    return {"value": val, "unit": UNIT, "cores": r["threads"], "kind": kind,
-            "sample": "%d step(s) of the full %d-particle scene (%d fluid), %d rebuild(s), %.1f s wall"
-                      % (r["steps"], r["particles"], r["fluid"], r["rebuilds"], r["seconds"])}
+        d, g, n, nf = RI.dam_break_files(td, seed=0, fluid=fluid, box=box)
+        if not RI.ref_available(3):
+            raise SystemExit("oracle/_ref/ref_mph3d is missing: build it with `make -C oracle ref REF=<reference>`")
+        r = RI.time_reference(d, g, 3, warmup, steps, threads, max_seconds=budget, timeout=3600,
+                              rebuild_at=rebuild_at)
+    r["workload"] = workload_name(fluid, box, 3, 0.005, n, nf)
+    r["value"] = r["fluid"] * r["steps"] / r["seconds"]
+    return r
+
+
+def cpu_baseline_entry(r, cores) -> dict:
+    return {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+            "physical_cores": cores["physical"], "logical_cpus": cores["logical"], "cpu_model": cores["model"],
+            "sample": "%d timed step(s) after %d warm-up step(s) of the full %d-particle scene (%d fluid), "
+                      "%d neighbour rebuild(s) inside the window, %.1f s wall, %d OpenMP thread(s); "
+                      "the reference's Mph_gcc3d flags (-O3 -fopenmp), compiled from its sources"
+                      % (r["steps"], r["warmup"], r["particles"], r["fluid"], r["rebuilds"], r["seconds"],
+                         r["threads"])}
 
 
 def run_reference_arm(args, rank, world):
+    """`--impl reference`: the reference's own CPU step on this line's workload,
+    all host threads, exactly --steps timed steps after --warmup untimed ones,
+    with one neighbour rebuild inside the window; then one step on one thread.
+    Rank 0 alone runs it (the other ranks exit without work)."""
     if rank != 0:
         return
-    sc = make_scene(args, 0)
-    steps = max(1, min(args.steps, args.ref_max_steps))
-    base = cpu_baseline(sc, args.ref_seconds, steps)
-    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+    from oracle import ref_inputs as RI
+    cores = RI.host_cores()
+    r = cpu_reference_sample(args, cores["logical"], args.steps, args.warmup, 1.0e30, args.steps // 2)
+    base = cpu_baseline_entry(r, cores)
+    if args.ref_single_steps > 0:
+        r1 = cpu_reference_sample(args, 1, args.ref_single_steps, 0, 1.0e30, -1)
+        base["single_thread"] = {"value": r1["value"], "unit": UNIT, "steps": r1["steps"],
+                                 "seconds": r1["seconds"], "rebuilds": r1["rebuilds"]}
+        base["thread_speedup"] = r["value"] / r1["value"]
+    ms = r["seconds"] * 1e3 / r["steps"]
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": r["warmup"], "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": workload_name(sc), "mode": "reference CPU (OpenMP)"},
+            "config": bench_config(r["workload"], "fp64"), "parallelism": "host CPU (OpenMP)",
             "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -591,13 +627,14 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mode", default="mixed_p64", choices=["fp64", "mixed", "mixed_p64"],
-                    help="headline form (all three are measured unless --only)")
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "mixed_p64"],
+                    help="headline form (default fp64: the reference's arithmetic, bit-exact); "
+                         "all three are measured unless --only")
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
-    ap.add_argument("--scene", default="dam", choices=["dam", "dam_mid", "dam_small"])
+    ap.add_argument("--scene", default="dam", choices=sorted(SCENES))
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch,two_fluid,output",
                     help="forms to measure (comma list); the headline --mode must be among them for a full line")
@@ -609,7 +646,7 @@ def main():
     ap.add_argument("--output-every", type=int, default=100, help="steps between VTK files written behind the step")
     ap.add_argument("--output-files", type=int, default=5)
     ap.add_argument("--two-fluid-n", type=int, default=200, help="fluid particles per axis of the two-fluid column")
-    ap.add_argument("--two-fluid-steps", type=int, default=50)
+    ap.add_argument("--two-fluid-steps", type=int, default=500)
     ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
     ap.add_argument("--batch-cpu-scenes", type=int, default=16)
     ap.add_argument("--batch-cpu-steps", type=int, default=200)
@@ -617,8 +654,10 @@ def main():
                     help="untimed steps before the warm-up, so the timed window sees the neighbour "
                          "rebuilds of the developed flow (a dam break at rest rebuilds rarely)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-seconds", type=float, default=25.0)
-    ap.add_argument("--ref-max-steps", type=int, default=5)
+    ap.add_argument("--ref-seconds", type=float, default=30.0,
+                    help="wall-clock bound of the cpu_baseline sample of the product's line")
+    ap.add_argument("--ref-single-steps", type=int, default=1,
+                    help="steps of the reference arm's one-thread figure (0: none)")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -645,7 +684,8 @@ def main():
     forms = {}
     for m, r in res.items():
         f = {"value": r["value"], "ms_per_step": r["ms"] / args.steps, "dominant_kernel": r["roofline"]["kernel"],
-             "kernels_ms_per_step": r["roofline"]["kernels_ms_per_step"], "rebuilds_in_timed_region": r["rebuilds"]}
+             "kernels_ms_per_step": r["roofline"]["kernels_ms_per_step"], "rebuilds_in_timed_region": r["rebuilds"],
+             "roofline_frac": r["roofline"]["frac"]}
         if "fp64" in res and m != "fp64":
             ref = res["fp64"]
             fl = ref["fluid"]
@@ -673,23 +713,24 @@ def main():
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(sc, args.ref_seconds, args.ref_max_steps)
+        from oracle import ref_inputs as RI
+        cores = RI.host_cores()
+        # bounded sample: the steps that fit in --ref-seconds, the first of them a neighbour rebuild
+        base = cpu_baseline_entry(cpu_reference_sample(args, cores["logical"], 1000, 1, args.ref_seconds, 0), cores)
 
     if rank == 0:
         n_all = sc.n
+        warm = max(args.warmup, 3)
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": max(args.warmup, 3), "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
+                "warmup": warm, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else "f32+f64",
                 "data": "synthetic (seeded generator)",
-                "config": {"workload": workload_name(sc), "mode": args.mode,
-                           "parallelism": "replicas" if world > 1 else "single GPU",
-                           "l2": "inputs larger than L2 (%.2f GB device state)" % (n_all * 260 / 1e9),
-                           "rebuilds_in_timed_region": head["rebuilds"],
-                           "timed_window": "steps %d-%d of the run (%d untimed steps, %d warm-up)"
-                                           % (args.preroll + max(args.warmup, 3) + 1,
-                                              args.preroll + max(args.warmup, 3) + args.steps, args.preroll,
-                                              max(args.warmup, 3)),
-                           "updates_all_particles_per_s": n_all * args.steps * world / (head["ms"] / 1e3)},
+                "config": bench_config(scene_workload(sc), args.mode),
+                "parallelism": "replicas (one scene per GPU)" if world > 1 else "single GPU",
+                "timed_window": "steps %d-%d of the run (%d untimed steps, %d warm-up), %d neighbour rebuild(s)"
+                                % (args.preroll + warm + 1, args.preroll + warm + args.steps, args.preroll, warm,
+                                   head["rebuilds"]),
+                "updates_all_particles_per_s": n_all * args.steps * world / (head["ms"] / 1e3),
                 "forms": forms, "roofline": head["roofline"], "cpu_baseline": base, "e2e": head["e2e"],
                 "gpu_launches": head["launches"], "clocks": head["clocks"]}
         print(json.dumps(line), flush=True)

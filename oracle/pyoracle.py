@@ -19,6 +19,8 @@ import numpy as np
 
 from mphexplicit_b200 import _native as N
 
+from .ref_inputs import ref_available, time_reference  # noqa: F401  (re-exported for tests and bench)
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
@@ -167,10 +169,6 @@ class Oracle:
 
 
 # ---------------------------------------------------------------------------
-def ref_available(dim: int) -> bool:
-    return os.path.exists(os.path.join(REF_DIR, "ref_mph%dd" % dim))
-
-
 def read_dump(path: str) -> dict:
     """Parse the binary dump written by oracle/ref_harness.cpp."""
     raw = open(path, "rb").read()
@@ -227,19 +225,6 @@ def run_reference(data_path: str, grid_path: str, dim: int, nsteps: int, virial:
         subprocess.run(cmd, check=True, cwd=td, env=env, timeout=timeout, stdout=subprocess.DEVNULL,
                        stderr=subprocess.DEVNULL)
         return read_dump(out)
-
-
-def time_reference(data_path: str, grid_path: str, dim: int, warmup: int, steps: int, threads: int,
-                   max_seconds: float = 1.0e30, timeout: float = 900) -> dict:
-    """Wall-clock the reference's step loop (ref_harness `time` command); stops
-    after the step that crosses max_seconds and reports the steps done."""
-    exe = os.path.join(REF_DIR, "ref_mph%dd" % dim)
-    with tempfile.TemporaryDirectory() as td:
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        r = subprocess.run([exe, "time", data_path, grid_path, str(warmup), str(steps), str(threads),
-                            repr(float(max_seconds))], check=True, cwd=td, env=env, timeout=timeout,
-                           capture_output=True, text=True)
-        return json.loads(r.stdout.strip().splitlines()[-1])
 
 
 def time_oracle(scene, warmup: int, steps: int, max_seconds: float = 1.0e30) -> dict:

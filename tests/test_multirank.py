@@ -30,9 +30,10 @@ def _worker(rank, world, port, q):
         ms = bench.max_over_ranks(10.0 + 3.0 * r, w)  # rank 1 is the slowest
         value = bench.job_value(1000, 5, w, ms)
         # the reference arm with a stand-in for the timed CPU sample
-        bench.cpu_baseline = lambda sc, seconds, steps: {"value": 123.0, "unit": bench.UNIT, "cores": 1,
-                                                          "kind": "port", "sample": "stand-in"}
-        args = Namespace(steps=5, warmup=3, ref_max_steps=1, ref_seconds=1.0, gpus=w, scene="dam_small")
+        bench.cpu_reference_sample = lambda a, threads, steps, warmup, budget, rebuild_at: {
+            "seconds": 1.0, "steps": steps, "warmup": warmup, "particles": 10, "fluid": 5,
+            "rebuilds": int(rebuild_at >= 0), "threads": threads, "workload": "stand-in", "value": 123.0}
+        args = Namespace(steps=5, warmup=3, ref_seconds=1.0, ref_single_steps=1, gpus=w, scene="dam_small")
         out = io.StringIO()
         with contextlib.redirect_stdout(out):
             bench.run_reference_arm(args, r, w)
@@ -45,6 +46,7 @@ def _worker(rank, world, port, q):
 
 def test_two_ranks_max_time_job_value_and_reference_arm():
     import json
+    import bench
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -63,5 +65,8 @@ def test_two_ranks_max_time_job_value_and_reference_arm():
         assert abs(res[r][1] - 1000 * 5 * 2 / 0.013) < 1e-6 * res[r][1]
     line = json.loads(res[0][2].strip())
     assert line["impl"] == "reference" and line["value"] == 123.0 and line["n_gpus"] == 2
+    assert line["steps"] == 5 and line["warmup"] == 3 and "1 neighbour rebuild" in line["cpu_baseline"]["sample"]
+    assert line["cpu_baseline"]["single_thread"]["steps"] == 1
+    assert line["config"] == bench.bench_config("stand-in", "fp64")
     assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert res[1][2] == ""  # the other ranks do no work and print nothing

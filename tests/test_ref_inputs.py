@@ -1,0 +1,55 @@
+"""The reference arm's inputs (oracle/ref_inputs.py) equal the product's scene.
+
+bench.py's CPU legs time the reference on files written by oracle/ref_inputs,
+which loads nothing of the product.  These tests pin that those files hold
+the same scene as the one the GPU arm steps: the same arrays element for
+element, the same *.data bytes and the same *.grid bytes as the product's
+writers; and that the timing command of the reference harness reports the
+steps, warm-up and the forced neighbour rebuild it was asked for (the rebuild
+is a timing device only: it reorders the particles, so the state after it is
+not compared with anything).
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from mphexplicit_b200 import scenes
+from oracle import ref_inputs as RI
+
+
+@pytest.mark.parametrize("fluid,box,seed", [((6, 5, 7), (14, 6, 12), 0), ((9, 4, 5), (20, 7, 9), 3)])
+def test_dam_break_arrays_equal_product_scene(fluid, box, seed):
+    sc = scenes.dam_break_3d(fluid=fluid, box=box, seed=seed)
+    p, h, t, x, v = RI.dam_break_arrays(fluid=fluid, box=box, seed=seed)
+    assert np.array_equal(t, sc.type)
+    assert np.array_equal(x, sc.xyz)
+    assert np.array_equal(v, sc.vel)
+    assert h["n"] == sc.n and h["l0"] == sc.header.particle_spacing
+    for d in range(3):
+        assert h["dmin"][d] == sc.header.domain_min[d] and h["dmax"][d] == sc.header.domain_max[d]
+    with tempfile.TemporaryDirectory() as td:
+        d1, g1 = os.path.join(td, "a.data"), os.path.join(td, "a.grid")
+        d2, g2 = os.path.join(td, "b.data"), os.path.join(td, "b.grid")
+        sc.write(d1, g1)                       # the product's writers (C ABI)
+        RI.write_data(d2, p)
+        RI.write_grid(g2, h, t, x, v)
+        assert open(d1, "rb").read() == open(d2, "rb").read()
+        assert open(g1, "rb").read() == open(g2, "rb").read()
+
+
+def test_host_cores():
+    c = RI.host_cores()
+    assert c["logical"] >= 1 and 1 <= c["physical"] <= c["logical"]
+
+
+@pytest.mark.skipif(not RI.ref_available(3), reason="reference build absent")
+def test_time_reference_forced_rebuild():
+    with tempfile.TemporaryDirectory() as td:
+        d, g, n, nf = RI.dam_break_files(td, fluid=(6, 5, 7), box=(14, 6, 12))
+        r = RI.time_reference(d, g, 3, 1, 3, 1, rebuild_at=1)
+        assert r["steps"] == 3 and r["warmup"] == 1 and r["rebuilds"] == 1
+        assert r["particles"] == n and r["fluid"] == nf
+        r = RI.time_reference(d, g, 3, 0, 2, 1)
+        assert r["rebuilds"] == 0
