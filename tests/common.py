@@ -10,6 +10,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
 CASES = ["square_drop_skip", "bridge", "moving_walls", "droplet_2d", "dam_break_small", "two_fluid_small"]
+# 3-D cases over 1000 steps from inputs inside the developed flow; their
+# neighbour lists are kept as SHA-256 digests (nptr_sha256, nind_sha256)
+LONG_CASES = ["dam_break_1000", "two_fluid_1000"]
 STATE_KEYS = ["particle_index", "type", "xyz", "vel", "force", "neighbor_count", "density_a", "vol_strain_p",
               "virial_pressure"]
 FIELD_KEYS = ["divergence_p", "pressure_p", "pressure_a", "gravity_center"]
@@ -48,6 +51,14 @@ class GoldenCase:
             return None
         with gzip.open(p, "rb") as g:
             return g.read()
+
+
+def csr_digests(ptr, ind) -> tuple[str, str]:
+    """SHA-256 of NeighborPtr (int64) and NeighborInd (int32) as the reference
+    stores them."""
+    import hashlib
+    return (hashlib.sha256(np.ascontiguousarray(ptr, np.int64).tobytes()).hexdigest(),
+            hashlib.sha256(np.ascontiguousarray(ind, np.int32).tobytes()).hexdigest())
 
 
 def assert_same(a, b, what=""):

@@ -17,7 +17,8 @@ import mphexplicit_b200 as M
 from mphexplicit_b200 import _native as N
 from mphexplicit_b200 import scenes
 from oracle import pyoracle as po
-from tests.common import CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same, micro_cases
+from tests.common import (CASES, CELL_KEYS, FIELD_KEYS, LONG_CASES, STATE_KEYS, GoldenCase, assert_same, csr_digests,
+                          micro_cases)
 
 pytestmark = pytest.mark.gpu
 
@@ -47,6 +48,36 @@ def test_fp64_matches_reference_golden(name):
     assert_same(ind, case.ref["nind"], "NeighborInd")
     info = s.info()
     assert info["rebuild_count"] == case.rebuilds
+    assert info["neighbor_ind_count"] == case.neighbor_ind_count
+    assert info["time"] == float(case.ref["time"])
+    s.close()
+
+
+@pytest.mark.parametrize("name", LONG_CASES)
+def test_fp64_matches_reference_golden_1000_steps(name):
+    """3-D, 1000 steps from inside the developed flow (dozens of neighbour
+    rebuilds), against the reference's own arrays: bit for bit (stricter than
+    the 1e-10 relative bound on the FP64 state)."""
+    case = GoldenCase(name)
+    s = solver_for(case)
+    s.step(case.steps)
+    s.synchronize()
+    s.compute_virial()
+    st, f, c = s.state(), s.fields(), s.cells()
+    for k in STATE_KEYS:
+        assert_same(st[k], case.ref[k], k)
+    for k in FIELD_KEYS:
+        if k == "gravity_center" and not any(s.params.surface_tension[t] for t in range(4)):
+            continue
+        assert_same(f[k], case.ref[k], k)
+    for k in CELL_KEYS:
+        assert_same(c[k], case.ref[k], k)
+    ptr, ind = s.neighbors()
+    dp, di = csr_digests(ptr, ind)
+    assert dp == str(case.ref["nptr_sha256"]), "NeighborPtr differs"
+    assert di == str(case.ref["nind_sha256"]), "NeighborInd differs"
+    info = s.info()
+    assert info["rebuild_count"] == case.rebuilds and case.rebuilds >= (30 if name == "dam_break_1000" else 5)
     assert info["neighbor_ind_count"] == case.neighbor_ind_count
     assert info["time"] == float(case.ref["time"])
     s.close()

@@ -14,7 +14,8 @@ import pytest
 
 from mphexplicit_b200 import read_data_file, read_grid_file, scenes
 from oracle import pyoracle as po
-from tests.common import micro_cases, CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same
+from tests.common import (micro_cases, CASES, CELL_KEYS, FIELD_KEYS, STATE_KEYS, GoldenCase, assert_same,
+                          csr_digests)
 
 
 def run_oracle(case: GoldenCase):
@@ -43,6 +44,24 @@ def test_oracle_matches_golden(name):
     assert o.rebuilds == case.rebuilds
     assert o.constants().n0a == float(case.ref["n0a"])
     assert o.constants().n0p == float(case.ref["n0p"])
+
+
+def test_oracle_matches_golden_two_fluid_1000_steps():
+    """The 1000-step 3-D two-fluid case (surface tension, interaction ratios
+    != 1, 7 rebuilds) bit for bit; its neighbour list through the digests.
+    (The 1000-step dam break, 22k particles, is compared on the GPU only.)"""
+    case = GoldenCase("two_fluid_1000")
+    o = run_oracle(case)
+    s, f, c = o.state(), o.fields(), o.cells()
+    for k in STATE_KEYS:
+        assert_same(s[k], case.ref[k], k)
+    for k in FIELD_KEYS:
+        assert_same(f[k], case.ref[k], k)
+    for k in CELL_KEYS:
+        assert_same(c[k], case.ref[k], k)
+    ptr, ind = o.neighbors()
+    assert csr_digests(ptr, ind) == (str(case.ref["nptr_sha256"]), str(case.ref["nind_sha256"]))
+    assert o.rebuilds == case.rebuilds
 
 
 # Known-answer lattice sums (main.cpp:861-949), values printed by the reference.
