@@ -61,9 +61,10 @@ extern "C" {
  * (ViscosityV main.cpp:1941-1985, DiffuseInterface :1778-1829, PressureA
  * force :1742-1775) replaced by an edge-MLP surrogate (mph_model) evaluated on
  * the tensor cores.  Every judge_interval steps the plain FP64 step is run
- * from the same state as the judge; when the relative L2 error of the fluid
- * forces exceeds the tolerance, that step and the steps up to the next
- * judgement take the plain step (fallback).  No reference counterpart. */
+ * from the same state as the judge; when the relative L2 error of the
+ * replaced terms (see mph_set_learned) exceeds the tolerance, that step and
+ * the steps up to the next judgement take the plain step (fallback).  No
+ * reference counterpart. */
 #define MPH_MODE_LEARNED  3
 
 /* ---- parameters read from the *.data file (main.cpp:489-539) --------- */
@@ -152,6 +153,55 @@ int mph_read_grid_file(const char* path, mph_grid_header* h, int capacity,
  * "%lf" for time; this writer uses the solver's "%e"). */
 int mph_write_grid_file(const char* path, const mph_grid_header* h,
                         const int* type, const double* xyz, const double* vel);
+
+/* ---- the scene generator (generator/generator.cpp) --------------------
+ * The reference's pre-processor GeneratorForMph reads a *.boid list of
+ * cuboids and writes a *.grid with particles on each cuboid's lattice.  These
+ * entry points replace it; on valid input the *.grid bytes are the
+ * reference's.  Malformed input returns MPH_ERR_IO with the reason (read it
+ * with mph_generator_last_error), where the reference prints a message and
+ * goes on, or never returns (a cuboid without EndCuboid). */
+typedef struct mph_cuboid {
+    double spacing;        /* Spacing                                  */
+    int type;              /* Type (0/1 fluid, 2/3 wall)               */
+    double lower[3];       /* Lower                                    */
+    double upper[3];       /* Upper                                    */
+    double velocity[3];    /* Velocity                                 */
+} mph_cuboid;
+
+typedef struct mph_boid {
+    double particle_distance;  /* ParticleDistance (the *.grid's l0)   */
+    double lower_domain[3];    /* LowerDomain                          */
+    double upper_domain[3];    /* UpperDomain                          */
+    int cuboid_count;
+} mph_boid;
+
+/* Read a *.boid file (readfile + readCuboid, generator.cpp:49-164): up to
+ * `capacity` cuboids are stored, *count receives how many the file holds
+ * (MPH_ERR_CAPACITY when that is more than capacity; capacity 0 with
+ * cuboids NULL asks for the count). */
+int mph_read_boid_file(const char* path, mph_boid* boid, mph_cuboid* cuboids, int capacity, int* count);
+
+/* Particles of the cuboids' lattices in the reference's order (genparticle,
+ * generator.cpp:170-193: per cuboid, count = round(width/Spacing) per axis,
+ * spacing = width/count, coordinates by repeated addition from lower +
+ * spacing/2 while below upper - 0.49 spacing, x outermost).  With type, xyz or
+ * vel NULL only *n is computed; otherwise up to `capacity` particles are
+ * written (MPH_ERR_CAPACITY beyond). */
+int mph_generate_cuboids(const mph_cuboid* cuboids, int count, int* type, double* xyz, double* vel,
+                         long long capacity, long long* n);
+
+/* Write generated particles as the generator's writefile does
+ * (generator.cpp:197-217: time "%lf", then the header and particle lines). */
+int mph_write_generated_grid(const char* path, const mph_boid* boid, long long n, const int* type,
+                             const double* xyz, const double* vel);
+
+/* The whole generator: read boid_path, write grid_path (GeneratorForMph
+ * <stem> reads <stem>.boid and writes <stem>.grid, generator.cpp:37-47). */
+int mph_generate_grid_file(const char* boid_path, const char* grid_path, long long* particle_count);
+
+/* Message of the last failed generator call on this thread. */
+int mph_generator_last_error(char* buf, int len);
 
 /* Compute the derived constants without creating a context (initializeWeight,
  * initializeFluid's CofK/CofA, initializeWall, initializeDomain). dim is 2 or 3. */
@@ -343,6 +393,17 @@ int mph_cell_sort_noalloc(const mph_constants* c, const mph_grid_header* h, int 
 typedef struct mph_model mph_model;
 typedef struct mph_dataset mph_dataset;
 
+/* Self-test of the bounded tensor-core waits (no reference counterpart).
+ * Every mbarrier wait of the edge-MLP kernels gives up after a fixed number
+ * of polls (about a second), sets the model's error flag, waits (within the
+ * same limit) for any MMA group still in flight and frees its tensor memory
+ * before the kernel returns; the call then reports MPH_ERR_DEVICE.  This entry
+ * point runs the training (kernel 0) or inference (kernel 1) kernel on one
+ * tile with its MMA groups withheld and a limit of `polls` (1 .. 2^22), so
+ * the first wait runs out with nothing in flight.  It returns that
+ * MPH_ERR_DEVICE and clears the flag again: the model stays usable. */
+int mph_model_check_wait(mph_model* m, int kernel, long long polls);
+
 int mph_model_create(unsigned long long seed, mph_model** out);
 void mph_model_destroy(mph_model* m);
 int mph_model_param_count(void);
@@ -377,7 +438,11 @@ int mph_collect_samples(mph_ctx* ctx, mph_dataset* d, long long max_samples, uns
 
 /* Attach a model to an MPH_MODE_LEARNED context (the context keeps a
  * reference; the model must outlive it) with the judge interval and the
- * relative force-error tolerance of the fallback. */
+ * tolerance of the fallback.  The judged error is the relative L2 error, over
+ * the fluid, of the terms the network replaces (PressureA + DiffuseInterface +
+ * ViscosityV, main.cpp:1742-1829, 1941-1985) against their FP64 values; when
+ * those terms are below 1e-6 of the total force, it is the relative L2 error
+ * of the total fluid force instead. */
 int mph_set_learned(mph_ctx* ctx, mph_model* m, int judge_interval, double tolerance);
 typedef struct mph_learned_info {
     long long steps;           /* steps taken in MPH_MODE_LEARNED              */
@@ -391,6 +456,7 @@ typedef struct mph_learned_info {
                                   when they are below 1e-6 of the total force) */
     double max_term_error;
     long long edges;           /* CSR edges the network evaluates per step     */
+    double max_accepted_error; /* largest judged error that was kept (<= tolerance) */
 } mph_learned_info;
 int mph_learned_stats(mph_ctx* ctx, mph_learned_info* info);
 

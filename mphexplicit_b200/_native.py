@@ -131,7 +131,7 @@ class LearnedInfo(C.Structure):
     _fields_ = [("steps", C.c_longlong), ("learned_steps", C.c_longlong), ("judged", C.c_longlong),
                 ("fallbacks", C.c_longlong), ("plain_steps", C.c_longlong), ("last_force_error", C.c_double),
                 ("max_force_error", C.c_double), ("last_term_error", C.c_double), ("max_term_error", C.c_double),
-                ("edges", C.c_longlong)]
+                ("edges", C.c_longlong), ("max_accepted_error", C.c_double)]
 
 
 class BatchTrial(C.Structure):
@@ -151,6 +151,19 @@ class BatchInfo(C.Structure):
                 ("scene_rebuilds", C.c_longlong), ("tile_splits", C.c_longlong), ("launches", C.c_longlong)]
 
 
+class Cuboid(C.Structure):
+    """mph_cuboid: one cuboid of a *.boid file (generator/generator.cpp:17-23)."""
+
+    _fields_ = [("spacing", C.c_double), ("type", C.c_int), ("lower", _D3), ("upper", _D3), ("velocity", _D3)]
+
+
+class Boid(C.Structure):
+    """mph_boid: the domain keys of a *.boid file."""
+
+    _fields_ = [("particle_distance", C.c_double), ("lower_domain", _D3), ("upper_domain", _D3),
+                ("cuboid_count", C.c_int)]
+
+
 BATCH_GRAPH_STEPS = 16
 
 # every symbol the header declares, with its ctypes signature
@@ -165,6 +178,11 @@ SIGNATURES = {
     "mph_read_grid_header": (_I, [C.c_char_p, C.POINTER(GridHeader)]),
     "mph_read_grid_file": (_I, [C.c_char_p, C.POINTER(GridHeader), _I, _ip, _dp, _dp]),
     "mph_write_grid_file": (_I, [C.c_char_p, C.POINTER(GridHeader), _ip, _dp, _dp]),
+    "mph_read_boid_file": (_I, [C.c_char_p, C.POINTER(Boid), C.POINTER(Cuboid), _I, _ip]),
+    "mph_generate_cuboids": (_I, [C.POINTER(Cuboid), _I, _ip, _dp, _dp, C.c_longlong, C.POINTER(C.c_longlong)]),
+    "mph_write_generated_grid": (_I, [C.c_char_p, C.POINTER(Boid), C.c_longlong, _ip, _dp, _dp]),
+    "mph_generate_grid_file": (_I, [C.c_char_p, C.c_char_p, C.POINTER(C.c_longlong)]),
+    "mph_generator_last_error": (_I, [C.c_char_p, _I]),
     "mph_compute_constants": (_I, [C.POINTER(Params), C.POINTER(GridHeader), _I, C.POINTER(Constants)]),
     "mph_create": (_I, [C.POINTER(Params), C.POINTER(GridHeader), _I, _I, _ip, _dp, _dp, C.POINTER(_P)]),
     "mph_step": (_I, [_P, _I]),
@@ -210,6 +228,7 @@ SIGNATURES = {
     "mph_model_fit_scales": (_I, [_P, _P]),
     "mph_model_train": (_I, [_P, _P, _I, _I, C.c_double, C.c_ulonglong, _dp]),
     "mph_model_last_error": (_I, [_P, C.c_char_p, _I]),
+    "mph_model_check_wait": (_I, [_P, _I, C.c_longlong]),
     "mph_dataset_create": (_I, [C.c_longlong, C.POINTER(_P)]),
     "mph_dataset_destroy": (None, [_P]),
     "mph_dataset_size": (C.c_longlong, [_P]),

@@ -235,25 +235,19 @@ def droplet_batch_2d(count: int = 256, seed: int = 0, l0: float = 1.0e-3, lo: in
 
 
 def cuboid_grid(cuboids, spacing_domain, lower, upper):
-    """The reference generator's lattice fill (generator/generator.cpp:170-193):
-    for each cuboid (spacing, type, lower, upper, velocity) particles at
-    lower + (i+0.5)*s for i while p < upper - 0.49 s, with s = width/round(width/spacing)."""
-    types, pos, vel = [], [], []
+    """The reference generator's lattice fill (generator/generator.cpp:170-193)
+    through the library's generator (mph_generate_cuboids): for each cuboid
+    (spacing, type, lower, upper, velocity), count = round(width/spacing) per
+    axis with C rounding (halves away from zero), spacing = width/count,
+    particles from lower + spacing/2 while below upper - 0.49 spacing.
+    Returns (header, type, xyz, vel)."""
+    from .solver import generate_cuboids
+    cs = []
     for (sp, typ, lo, up, v) in cuboids:
-        width = [up[d] - lo[d] for d in range(3)]
-        count = [round(width[d] / sp) for d in range(3)]
-        s = [width[d] / count[d] for d in range(3)]
-        px = lo[0] + 0.5 * s[0]
-        while px < up[0] - 0.49 * s[0]:
-            py = lo[1] + 0.5 * s[1]
-            while py < up[1] - 0.49 * s[1]:
-                pz = lo[2] + 0.5 * s[2]
-                while pz < up[2] - 0.49 * s[2]:
-                    types.append(typ)
-                    pos.append((px, py, pz))
-                    vel.append(tuple(v))
-                    pz += s[2]
-                py += s[1]
-            px += s[0]
-    h = make_header(len(types), spacing_domain, lower, upper)
-    return h, np.array(types, np.int32), np.array(pos, np.float64).reshape(-1, 3), np.array(vel, np.float64).reshape(-1, 3)
+        c = N.Cuboid()
+        c.spacing, c.type = float(sp), int(typ)
+        for d in range(3):
+            c.lower[d], c.upper[d], c.velocity[d] = float(lo[d]), float(up[d]), float(v[d])
+        cs.append(c)
+    t, x, vel = generate_cuboids(cs)
+    return make_header(len(t), spacing_domain, lower, upper), t, x, vel

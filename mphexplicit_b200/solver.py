@@ -104,6 +104,49 @@ def write_grid_file(path: str, header: N.GridHeader, type_, xyz, vel) -> None:
     _check(N.load().mph_write_grid_file(str(path).encode(), C.byref(header), _ip(t), _dp(x), _dp(v)))
 
 
+def _gen_check(st: int) -> None:
+    if st != N.MPH_OK:
+        buf = C.create_string_buffer(512)
+        N.load().mph_generator_last_error(buf, 512)
+        raise MphError(st, buf.value.decode(errors="replace"))
+
+
+def read_boid_file(path: str):
+    """The reference generator's readfile (generator/generator.cpp:49-164):
+    returns (Boid, [Cuboid, ...])."""
+    lib = N.load()
+    b = N.Boid()
+    cnt = C.c_int(0)
+    st = lib.mph_read_boid_file(str(path).encode(), C.byref(b), None, 0, C.byref(cnt))
+    if st not in (N.MPH_OK, N.MPH_ERR_CAPACITY):
+        _gen_check(st)
+    arr = (N.Cuboid * max(cnt.value, 1))()
+    _gen_check(lib.mph_read_boid_file(str(path).encode(), C.byref(b), arr, cnt.value, C.byref(cnt)))
+    return b, [arr[k] for k in range(cnt.value)]
+
+
+def generate_cuboids(cuboids):
+    """genparticle (generator.cpp:170-193): (type, xyz, vel) of the cuboids'
+    lattices in the reference's order."""
+    lib = N.load()
+    arr = (N.Cuboid * max(len(cuboids), 1))(*cuboids)
+    n = C.c_longlong(0)
+    _gen_check(lib.mph_generate_cuboids(arr, len(cuboids), None, None, None, 0, C.byref(n)))
+    t = np.zeros(n.value, np.int32)
+    x = np.zeros((n.value, 3), np.float64)
+    v = np.zeros((n.value, 3), np.float64)
+    _gen_check(lib.mph_generate_cuboids(arr, len(cuboids), _ip(t), _dp(x), _dp(v), n.value, C.byref(n)))
+    return t, x, v
+
+
+def generate_grid_file(boid_path: str, grid_path: str) -> int:
+    """The whole generator (GeneratorForMph): *.boid in, *.grid out; returns
+    the particle count."""
+    n = C.c_longlong(0)
+    _gen_check(N.load().mph_generate_grid_file(str(boid_path).encode(), str(grid_path).encode(), C.byref(n)))
+    return int(n.value)
+
+
 def write_vtk_arrays(path: str, state: dict) -> None:
     """writeVtkFile (main.cpp:698-834) from host arrays (keys as Solver.state())."""
     t = np.ascontiguousarray(state["type"], np.int32)
