@@ -36,6 +36,15 @@ using tc::core_off;
 
 constexpr long long kWaitLimit = 1ll << 22;  // mbarrier polls before a wait is abandoned (~1 s)
 
+// Wait control of the MLP kernels: the poll limit of every mbarrier wait, and
+// whether the MMA groups are issued (always, except in the wait self-test of
+// model_check_wait, where withholding them makes the first wait run out with
+// nothing in flight).
+struct WaitCtl {
+    long long limit;
+    int issue;
+};
+
 // shared memory of the training kernel (bytes)
 constexpr int S_W = 0;  // packed image: W1, W2, W3, W4 (core layout), b1..b4 (FP32)
 constexpr int S_X = 75776;
@@ -215,7 +224,7 @@ __device__ __forceinline__ float warp_sum(float x) {
 __global__ void __launch_bounds__(128, 1)
 k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ samples,
             const long long* __restrict__ order, long long n, Scales sc, float* __restrict__ gpart,
-            double* __restrict__ lossp, int* __restrict__ err) {
+            double* __restrict__ lossp, int* __restrict__ err, WaitCtl wc) {
     extern __shared__ __align__(128) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     {
@@ -252,19 +261,27 @@ k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 
     uint32_t phase = 0;
     bool ok = true;
+    bool inflight = false;        // a committed MMA group whose completion was not seen
+    uint32_t failed_parity = 0;
     auto run = [&](auto&& issue) {
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue();
-            tc::commit(mb);
+            if (wc.issue) {
+                issue();
+                tc::commit(mb);
+            }
         }
-        const bool done = tc::mbar_wait(mb, phase, kWaitLimit);
-        phase ^= 1u;
+        const bool done = tc::mbar_wait(mb, phase, wc.limit);
         tc::fence_after_sync();
         ok = __syncthreads_and(done) != 0;
+        if (!ok) {
+            inflight = wc.issue != 0;
+            failed_parity = phase;
+        }
+        phase ^= 1u;
     };
 
     double acc_loss = 0.0;
@@ -404,6 +421,9 @@ k_mlp_train(const uint8_t* __restrict__ image, const float4* __restrict__ sample
             for (int q = 0; q < KOUT; ++q) gp[OFF_B4 + q] = q < NOUT ? acc_b4[q] : 0.f;
     }
     if (tid == 0) lossp[blockIdx.x] = acc_loss;
+    // after a wait that ran out: wait, again within the limit, for the MMA
+    // group still in flight before its TMEM is given back
+    if (!ok && inflight) (void)tc::mbar_wait(mb, failed_parity, wc.limit);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_free(tb, 512);
@@ -440,7 +460,7 @@ __device__ __forceinline__ bool wg_sync_and(int id, bool v) {
 template <int SRC>
 __global__ void __launch_bounds__(128 * I_WG, 1)
 k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ samples, long long n, EdgeSource es,
-            Scales sc, float4* __restrict__ out, int* __restrict__ err) {
+            Scales sc, float4* __restrict__ out, int* __restrict__ err, WaitCtl wc) {
     extern __shared__ __align__(128) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, row = tid & 127;
     {
@@ -473,19 +493,27 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
 
     uint32_t phase = 0;
     bool ok = true;
+    bool inflight = false;        // a committed MMA group whose completion was not seen
+    uint32_t failed_parity = 0;
     auto run = [&](auto&& issue) {
         tc::fence_async_smem();
         tc::fence_before_sync();
         wg_sync(bar);
         if (row == 0) {
             tc::fence_after_sync();
-            issue();
-            tc::commit(mb);
+            if (wc.issue) {
+                issue();
+                tc::commit(mb);
+            }
         }
-        const bool done = tc::mbar_wait(mb, phase, kWaitLimit);
-        phase ^= 1u;
+        const bool done = tc::mbar_wait(mb, phase, wc.limit);
         tc::fence_after_sync();
         ok = wg_sync_and(bar, done);
+        if (!ok) {
+            inflight = wc.issue != 0;
+            failed_parity = phase;
+        }
+        phase ^= 1u;
     };
     const long long rows = SRC == 0 ? n : es.ne;
     const long long ntiles = (rows + TILE - 1) / TILE;
@@ -590,6 +618,9 @@ k_mlp_infer(const uint8_t* __restrict__ image, const float4* __restrict__ sample
         }
     }
     if (!ok && row == 0) atomicExch(err, 1);
+    // after a wait that ran out: wait, again within the limit, for this
+    // warpgroup's MMA group still in flight before the TMEM is given back
+    if (!ok && inflight) (void)tc::mbar_wait(mb, failed_parity, wc.limit);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) tc::tmem_free(*tslot, 128 * I_WG);
@@ -751,7 +782,8 @@ int model_grad(Model* m, const float4* samples, const long long* order, long lon
     }
     const long long ntiles = (n + TILE - 1) / TILE;
     const int ctas = (int)std::min<long long>(m->ctas, ntiles);
-    k_mlp_train<<<ctas, 128, S_TRAIN, m->stream>>>(m->image, samples, order, n, m->sc, m->gpart, m->lossp, m->err);
+    k_mlp_train<<<ctas, 128, S_TRAIN, m->stream>>>(m->image, samples, order, n, m->sc, m->gpart, m->lossp, m->err,
+                                                   WaitCtl{kWaitLimit, 1});
     MTRY(cudaGetLastError());
     k_grad_reduce<<<(NPARAM + 255) / 256, 256, 0, m->stream>>>(m->gpart, ctas, (float)(2.0 / (3.0 * (double)n)),
                                                                m->grad);
@@ -782,7 +814,8 @@ int model_predict(Model* m, const float4* samples, long long n, float4* out, std
     const long long ntiles = (n + TILE - 1) / TILE;
     const int ctas = (int)std::min<long long>(m->ctas, (ntiles + I_WG - 1) / I_WG);
     EdgeSource es{};
-    k_mlp_infer<0><<<ctas, 128 * I_WG, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err);
+    k_mlp_infer<0><<<ctas, 128 * I_WG, S_INFER, m->stream>>>(m->image, samples, n, es, m->sc, out, m->err,
+                                                              WaitCtl{kWaitLimit, 1});
     MTRY(cudaGetLastError());
     return check_flag(m, err);
 }
@@ -793,13 +826,46 @@ int model_apply_edges(Model* m, const EdgeSource& src, float4* out, cudaStream_t
     if (src.ne <= 0) return 0;
     const long long ntiles = (src.ne + TILE - 1) / TILE;
     const int ctas = (int)std::min<long long>(m->ctas, (ntiles + I_WG - 1) / I_WG);
-    k_mlp_infer<1><<<ctas, 128 * I_WG, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err);
+    k_mlp_infer<1><<<ctas, 128 * I_WG, S_INFER, s>>>(m->image, nullptr, 0, src, m->sc, out, m->err,
+                                                     WaitCtl{kWaitLimit, 1});
     MTRY(cudaGetLastError());
     if (launches) *launches = 1;
     return 0;
 }
 
 int model_error_flag(Model* m, std::string* err) { return check_flag(m, err); }
+
+int model_check_wait(Model* m, int which, long long polls, std::string* err) {
+    if (polls < 1 || polls > kWaitLimit || (which != 0 && which != 1)) {
+        if (err) *err = "bad arguments";
+        return -1;
+    }
+    // one tile of zero samples; the kernel's first wait runs out after `polls`
+    // polls because no MMA group is issued, so nothing is in flight when it
+    // sets the error flag and frees its TMEM
+    float4* buf = nullptr;  // 3 float4 per sample (TILE samples), then TILE outputs
+    const size_t bytes = (size_t)TILE * 4 * sizeof(float4);
+    MTRY(cudaMalloc(&buf, bytes));
+    float4* samples = buf;
+    cudaError_t e = cudaMemsetAsync(buf, 0, bytes, m->stream);
+    if (e == cudaSuccess) {
+        if (which == 0)
+            k_mlp_train<<<1, 128, S_TRAIN, m->stream>>>(m->image, samples, nullptr, TILE, m->sc, m->gpart, m->lossp,
+                                                         m->err, WaitCtl{polls, 0});
+        else
+            k_mlp_infer<0><<<1, 128 * I_WG, S_INFER, m->stream>>>(m->image, samples, TILE, EdgeSource{}, m->sc,
+                                                                   buf + 3 * TILE, m->err, WaitCtl{polls, 0});
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    cudaFree(buf);
+    MTRY(e);
+    const int rc = check_flag(m, err);
+    // the model stays usable: clear the flag the self-test raised
+    MTRY(cudaMemsetAsync(m->err, 0, sizeof(int), m->stream));
+    MTRY(cudaStreamSynchronize(m->stream));
+    return rc;
+}
 
 }  // namespace mlp
 }  // namespace mph

@@ -839,16 +839,23 @@ static int step_learned(mph_ctx* ctx, int nsteps) {
                 ++L.info.judged;
                 L.info.last_force_error = e;
                 L.info.max_force_error = std::max(L.info.max_force_error, e);
-                // the replaced terms' own relative error, where they are not
-                // negligible against the total force (a fluid at rest has none)
+                // The judged error is the replaced terms' own relative error
+                // (the network's output against the FP64 PressureA +
+                // DiffuseInterface + ViscosityV it stands for); where those
+                // terms are negligible against the total force (a fluid at
+                // rest has none) it is the error of the total force.
+                double judged_error = e;
                 if (L.h_sums[2] > 1e-12 * L.h_sums[1]) {
                     const double te = std::sqrt(L.h_sums[0] / L.h_sums[2]);
                     L.info.last_term_error = te;
                     L.info.max_term_error = std::max(L.info.max_term_error, te);
+                    judged_error = te;
                 } else {
                     L.info.last_term_error = 0.0;
                 }
-                if (!(e <= L.tol)) {  // fall back: take the judge's step
+                if (judged_error <= L.tol)
+                    L.info.max_accepted_error = std::max(L.info.max_accepted_error, judged_error);
+                if (!(judged_error <= L.tol)) {  // fall back: take the judge's step
                     use = false;
                     ++L.info.fallbacks;
                     ++L.info.plain_steps;

@@ -125,6 +125,11 @@ extern "C" int mph_model_predict(mph_model* m, const float* samples, long long n
     return MPH_OK;
 }
 
+extern "C" int mph_model_check_wait(mph_model* m, int kernel, long long polls) {
+    if (!m || (kernel != 0 && kernel != 1) || polls < 1 || polls > (1ll << 22)) return MPH_ERR_ARG;
+    return map_rc(mph::mlp::model_check_wait(&m->m, kernel, polls, &m->err));
+}
+
 extern "C" int mph_model_last_error(mph_model* m, char* buf, int len) {
     if (!m || !buf || len <= 0) return MPH_ERR_ARG;
     std::snprintf(buf, (size_t)len, "%s", m->err.c_str());

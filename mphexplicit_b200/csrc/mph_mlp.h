@@ -101,6 +101,11 @@ int model_apply_edges(Model* m, const EdgeSource& src, float4* out, cudaStream_t
                       std::string* err);
 // nonzero (and *err set) when a tensor-core wait of an MLP kernel gave up
 int model_error_flag(Model* m, std::string* err);
+// Self-test of the bounded waits: the training (which 0) or inference
+// (which 1) kernel on one tile with its MMA groups withheld and a wait limit
+// of `polls`; returns what a timed-out wait returns (-5, *err set) once the
+// kernel has freed its TMEM, and clears the model's error flag.
+int model_check_wait(Model* m, int which, long long polls, std::string* err);
 
 }  // namespace mlp
 }  // namespace mph

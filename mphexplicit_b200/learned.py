@@ -114,6 +114,16 @@ class Model:
                                           C.byref(loss)), self.handle)
         return loss.value
 
+    def check_wait(self, kernel: int, polls: int) -> tuple[int, str]:
+        """mph_model_check_wait: the training (0) or inference (1) kernel with
+        its tensor-core work withheld and a wait limit of `polls`; returns the
+        status (MPH_ERR_DEVICE when the bounded wait ran out as it should) and
+        the model's error message."""
+        st = self._lib.mph_model_check_wait(self.handle, int(kernel), int(polls))
+        buf = C.create_string_buffer(256)
+        self._lib.mph_model_last_error(self.handle, buf, 256)
+        return st, buf.value.decode(errors="replace")
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             self._lib.mph_model_destroy(self.handle)

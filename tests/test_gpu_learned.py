@@ -40,6 +40,29 @@ def test_mlp_forward_and_gradient_match_oracle(n):
     m.close()
 
 
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_bounded_wait_runs_out_and_model_stays_usable(kernel):
+    """The training (0) and inference (1) kernels with their MMA groups
+    withheld and a wait limit of 64 polls: the mbarrier wait runs out with
+    nothing in flight, the kernel sets the error flag and frees its tensor
+    memory, the call reports MPH_ERR_DEVICE; the same model then computes the
+    same outputs and gradients as before."""
+    from mphexplicit_b200 import _native as N
+    m = LR.Model(seed=0)
+    p = O.random_params(7)
+    m.set_params(p)
+    m.set_scales(0.7, 3.0)
+    s = O.random_samples(300, 5)
+    f0 = m.predict(s)
+    g0, l0 = m.gradient(s)
+    st, msg = m.check_wait(kernel, 64)
+    assert st == N.MPH_ERR_DEVICE and "timed out" in msg, (st, msg)
+    assert np.array_equal(m.predict(s), f0)
+    g1, l1 = m.gradient(s)
+    assert np.array_equal(g1, g0) and l1 == l0
+    m.close()
+
+
 def test_mlp_params_round_trip_and_padding():
     m = LR.Model(seed=3)
     p = m.params()
@@ -102,6 +125,27 @@ def test_learned_fallback_everywhere_is_the_fp64_step():
     ref, _ = _run(sc, "fp64", 30)
     got, stats = _run(sc, "learned", 30, m, judge=10, tol=1e-300)
     assert stats["learned_steps"] == 0 and stats["fallbacks"] == 3 and stats["plain_steps"] == 30
+    for k in ("xyz", "vel"):
+        assert np.array_equal(by_original_id(got, k), by_original_id(ref, k))
+    m.close()
+
+
+def test_untrained_model_falls_back():
+    """An untrained network (random weights) on a flowing scene: every judgement
+    sees the replaced terms' error far over the tolerance and takes the plain
+    step, so the run equals the FP64 step bit for bit."""
+    sc = _scene()
+    s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=sc.dim, mode="fp64")
+    s.step(40)  # into the flow: the replaced (viscous) terms are non-zero
+    st = s.state()
+    s.close()
+    o = np.argsort(st["particle_index"], kind="stable")
+    flowing = scenes.Scene(sc.name, sc.dim, sc.params, sc.header, st["type"][o], st["xyz"][o], st["vel"][o], 30)
+    m = LR.Model(seed=4)
+    ref, _ = _run(flowing, "fp64", 30)
+    got, stats = _run(flowing, "learned", 30, m, judge=10, tol=1e-2)
+    assert stats["judged"] == 3 and stats["fallbacks"] == 3 and stats["learned_steps"] == 0, stats
+    assert stats["last_term_error"] > 1e-2 and stats["max_accepted_error"] == 0.0, stats
     for k in ("xyz", "vel"):
         assert np.array_equal(by_original_id(got, k), by_original_id(ref, k))
     m.close()
