@@ -260,7 +260,10 @@ int mph_get_cells(mph_ctx* ctx, int* cell_index, int* fluid_begin, int* fluid_en
 int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long long ind_capacity);
 
 /* Virial stress and pressure at particles (calculateVirialStressAtParticle,
- * main.cpp:2057-2302), computed on the device from the current state. */
+ * main.cpp:2057-2302), computed on the device from the current state: in the
+ * reference's FP64 order for MPH_MODE_FP64 / MPH_MODE_LEARNED (bit-identical),
+ * with FP32 pair terms over the form's own neighbour table for the mixed
+ * forms (output only; close to the FP64 values, not equal). */
 int mph_compute_virial(mph_ctx* ctx);
 
 /* Output files in the reference formats and in sorted order:
@@ -367,10 +370,16 @@ int mph_check_exact_division(long long n, unsigned long long seed, long long* mi
  * the caller; c comes from mph_compute_constants, h gives the domain origin;
  * stream is a cudaStream_t (NULL: the legacy default stream) and the call is
  * asynchronous on it.  The sort's scratch is a fixed static device array of
- * 2^21 ints (8 MiB, held by every GPU that loads the library until exit), so
- * n must be below 2^20 (1,048,576); larger n returns MPH_ERR_CAPACITY.  The
- * first call on a device looks up that array's device address (set-up), so
- * make that first call before any stream capture.  All calls share the one
+ * 2^21 ints (8 MiB), so n must be below 2^20 (1,048,576); larger n returns
+ * MPH_ERR_CAPACITY.  The first call on a device is its set-up: it looks up
+ * that array's device address (once per device for the life of the process),
+ * and under CUDA's lazy module loading (the default) it is also the call that
+ * loads the library's module, and with it the 8 MiB array, onto that device,
+ * which then holds it until the process exits.  Callers with a fixed device
+ * budget should therefore make the first call during their own set-up, and
+ * before any stream capture.  A process that resets a device
+ * (cudaDeviceReset) must not call this entry point on it again: the address
+ * looked up at set-up belongs to the context that was reset.  All calls share the one
  * scratch array: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller.  Allocates nothing
  * (no cudaMalloc, cudaFree or allocating library call). */

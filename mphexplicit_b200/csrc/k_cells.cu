@@ -12,6 +12,7 @@
 //   * neighbour list:  main.cpp:1329-1596, same stencil order, self included,
 //                      wall particles without a fluid neighbour get no list.
 // Compiled with -fmad=false so the distance test is not FMA-contracted.
+#include <cmath>
 #include "mph_internal.h"
 
 namespace mph {
@@ -150,10 +151,19 @@ __global__ void k_reorder(int n, const int* __restrict__ vals, const int* __rest
 // sublist: a particle moves at most MARGIN/2 between builds (the rebuild test
 // of main.cpp:1086-1108), so every pair within RadiusP until the next build is
 // in it, and a sum over the pairs within RadiusP visits them in list order.
+//
+// Prefilter (pos32 != nullptr): FP32 positions relative to the domain origin
+// (k_pos32) give a displacement within the bound of make_prefilter of the one
+// the exact FP64 test computes, so a candidate whose FP32 distance squared
+// exceeds pf.r2_hi cannot pass that test and is skipped; every other candidate
+// takes the exact test.  The list is therefore the same, entry for entry.  An
+// axis with fewer than 4 cells contributes nothing to the FP32 distance (its
+// minimum image need not be the neighbouring cell's), which only keeps more
+// candidates.
 __global__ void __launch_bounds__(256)
-k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restrict__ keys,
-                const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist,
-                int cap, int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s,
+k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __restrict__ pos32, Prefilter pf,
+                const int* __restrict__ keys, const int* __restrict__ cellstart, int* __restrict__ ncount,
+                int* __restrict__ nlist, int cap, int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s,
                 StepScalars* __restrict__ scal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -162,22 +172,23 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
     const int icy = (ci / c.cc[2]) % c.cc[1];
     const int icz = ci % c.cc[2];
     int jc[3][3];
+    float jo[3][3];  // FP32 image offset of each stencil slot (0, or -+ the domain width where it wraps)
     const int ic[3] = {icx, icy, icz};
     int jmin[3], w[3];
     for (int d = 0; d < 3; ++d) {
         const int r = c.range[d];
         w[d] = 2 * r + 1;
-        for (int j = 0; j < w[d]; ++j) jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
+        for (int j = 0; j < w[d]; ++j) {
+            const int raw = ic[d] - r + j;
+            jc[d][j] = (raw % c.cc[d] + c.cc[d]) % c.cc[d];
+            jo[d][j] = raw < 0 ? -pf.width[d] : (raw >= c.cc[d] ? pf.width[d] : 0.0f);
+        }
         const int b = (2 * r) - (ic[d] + r) % c.cc[d];       // main.cpp:1376-1381
         jmin[d] = b > 0 ? b : 0;
     }
-    int cells[27];
-    int nc = 0;
-    for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-        for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-            for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz)
-                cells[nc++] = cell_id(c, jc[0][jx % w[0]], jc[1][jy % w[1]], jc[2][jz % w[2]]);
     const double4 pi = pos[i];
+    const bool filter = pos32 != nullptr;
+    const float4 pf_i = filter ? pos32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int wall_begin = cellstart[c.tot], wall_end = cellstart[2 * c.tot];
     const size_t n = (size_t)c.n;
     int cnt = 0, cnt_s = 0;
@@ -185,24 +196,38 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
     for (int kind = 0; kind < 2; ++kind) {
         if (kind == 1 && wall_begin <= i && i < wall_end && cnt == 0) break;  // main.cpp:1416
         const int off = kind ? c.tot : 0;
-        for (int k = 0; k < nc; ++k) {
-            const int b = cellstart[cells[k] + off], e = cellstart[cells[k] + off + 1];
-            for (int j = b; j < e; ++j) {
-                const double4 pj = pos[j];
-                const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-                const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-                const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
-                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-                if (r2 <= c.rm2) {
-                    if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
-                    cnt++;
-                    if (short_list && r2 <= c.rs2) {
-                        if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
-                        cnt_s++;
+        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                    const int sx = jx % w[0], sy = jy % w[1], sz = jz % w[2];
+                    const int cell = cell_id(c, jc[0][sx], jc[1][sy], jc[2][sz]);
+                    const float ox = pf.use[0] ? jo[0][sx] - pf_i.x : 0.f;
+                    const float oy = pf.use[1] ? jo[1][sy] - pf_i.y : 0.f;
+                    const float oz = pf.use[2] ? jo[2][sz] - pf_i.z : 0.f;
+                    const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                    for (int j = b; j < e; ++j) {
+                        if (filter) {
+                            const float4 q = pos32[j];
+                            const float fx = pf.use[0] ? q.x + ox : 0.f;
+                            const float fy = pf.use[1] ? q.y + oy : 0.f;
+                            const float fz = pf.use[2] ? q.z + oz : 0.f;
+                            if (fx * fx + fy * fy + fz * fz > pf.r2_hi) continue;
+                        }
+                        const double4 pj = pos[j];
+                        const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+                        const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+                        const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+                        const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                        if (r2 <= c.rm2) {
+                            if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
+                            cnt++;
+                            if (short_list && r2 <= c.rs2) {
+                                if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
+                                cnt_s++;
+                            }
+                        }
                     }
                 }
-            }
-        }
     }
     ncount[i] = cnt;
     atomicMax(&scal->max_neighbors, cnt);
@@ -212,6 +237,17 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const int* __restri
         atomicMax(&scal->max_short, cnt_s);
         if (cnt_s > cap_s) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
     }
+}
+
+// FP32 copies of the positions relative to the domain origin, for the list
+// build's prefilter: Mod(x - dmin, W) in [0, W), the coordinate of the
+// particle's image in the cell its CellId names (main.cpp:96-100).
+__global__ void k_pos32(SimConst c, const double4* __restrict__ pos, float4* __restrict__ pos32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const double4 p = pos[i];
+    pos32[i] = make_float4((float)omod(p.x - c.dmin[0], c.width[0]), (float)omod(p.y - c.dmin[1], c.width[1]),
+                           (float)omod(p.z - c.dmin[2], c.width[2]), 0.f);
 }
 
 __global__ void k_pack3(int n, const double4* __restrict__ src, double* __restrict__ dst) {
@@ -279,11 +315,41 @@ void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, cons
                                                type_out, pos_out, vel_out, snap);
 }
 
-void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys, const int* cellstart,
-                          int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
-                          StepScalars* scal, cudaStream_t s) {
-    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, keys, cellstart, ncount, nlist, cap, ncount_s,
-                                                     nlist_s, cap_s, scal);
+// Bound of the prefilter (see k_neighbor_list).  An FP32 coordinate in
+// [0, W) is within 2^-24 W of its FP64 value (two coordinates: 2 * 2^-24 W);
+// a component is formed as q + (offset - p_i) with |offset - p_i| < 2W
+// (2 * 2^-24 W more) and a small result (less than 2^-24 W more), so each
+// component is within e = 5 * 2^-24 * W of the FP64 minimum-image
+// displacement (W rounded to FP32 for the offset adds 2^-24 W), which is
+// itself within 2^-50 W of the true one.  The FP32 distance is then within
+// sqrt(3) e < 2e of the FP64 one, and the FP32 sum of squares within a factor
+// 1 + 2^-21 of its exact value: a candidate the FP64 test accepts (r <= rm)
+// has an FP32 distance squared below (rm + 2e)^2 (1 + 2^-20), rounded up to
+// the next float.  e is taken as 8 * 2^-24 * W for room.
+Prefilter make_prefilter(const SimConst& c) {
+    Prefilter pf{};
+    double wmax = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        pf.use[d] = c.cc[d] >= 4 && c.range[d] == 1;
+        pf.width[d] = (float)c.width[d];
+        if (pf.use[d]) wmax = std::fmax(wmax, c.width[d]);
+    }
+    const double e = 8.0 * std::ldexp(wmax, -24);
+    const double rm = std::sqrt(c.rm2);
+    const double t = (rm + 2.0 * e) * (rm + 2.0 * e) * (1.0 + std::ldexp(1.0, -20));
+    pf.r2_hi = std::nextafter((float)t, 3.0e38f);
+    return pf;
+}
+
+void launch_pos32(const SimConst& c, const double4* pos, float4* pos32, cudaStream_t s) {
+    k_pos32<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, pos32);
+}
+
+void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* keys,
+                          const int* cellstart, int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s,
+                          int cap_s, StepScalars* scal, cudaStream_t s) {
+    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, pos32, make_prefilter(c), keys, cellstart, ncount,
+                                                     nlist, cap, ncount_s, nlist_s, cap_s, scal);
 }
 
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s) {

@@ -39,11 +39,19 @@ __device__ __forceinline__ double omod_fast(double x, double w) {
     return (x >= 0.0 && x < 0.75 * w) ? x : omod(x, w);
 }
 
+// The same Mod with the range test as one unsigned compare of x's bits
+// against those of 0.75 w (SimConst::q75_bits): equal to omod_fast for every x
+// except -0.0, which takes omod and gives +0.0 instead of -0.0; the callers
+// then subtract half_width (non-zero), so their results are the same.
+__device__ __forceinline__ double omod_q(double x, double w, unsigned long long q75) {
+    return ((unsigned long long)__double_as_longlong(x) < q75) ? x : omod(x, w);
+}
+
 // Minimum-image displacement x_j - x_i (main.cpp:1680 and every sweep).
 __device__ __forceinline__ void disp(const SimConst& c, const double4& pi, const double4& pj, double* x) {
-    x[0] = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-    x[1] = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-    x[2] = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+    x[0] = omod_q(pj.x - pi.x + c.half_width[0], c.width[0], c.q75_bits[0]) - c.half_width[0];
+    x[1] = omod_q(pj.y - pi.y + c.half_width[1], c.width[1], c.q75_bits[1]) - c.half_width[1];
+    x[2] = omod_q(pj.z - pi.z + c.half_width[2], c.width[2], c.q75_bits[2]) - c.half_width[2];
 }
 
 // Kernel shapes, main.cpp:214-284, with q = r/h computed by division.
@@ -185,31 +193,33 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-        const bool in_a = DA && (c.ra2 - r2 >= 0);
-        const bool in_p = c.rp2 - r2 >= 0;
-        const bool in_g = ST && (c.rg2 - r2 >= 0);
+        // R*R - r2 >= 0 (main.cpp:1683 and the other density sums) is r2 <= R*R:
+        // with gradual underflow a - b is zero only when a == b, and its sign exact
+        const bool in_a = DA && (r2 <= c.ra2);
+        const bool in_p = r2 <= c.rp2;
+        const bool in_g = ST && (r2 <= c.rg2);
         if (!(in_a || in_p || in_g)) continue;
         const double r = sqrt(r2);
         double ratio = 1.0;
         if (RATIO) ratio = c.ratio[ti][type_of(pj)];
-        const double qa = div_rn(r, c.ra, c.inv_ra);
+        const double qa = div_rs(r, c.ra, c.inv_ra);
         if (in_a) {
             const double w = RATIO ? ratio * s_wa(c, qa) : s_wa(c, qa);
             sum_a += w;
         }
         if (ST && in_g) {
-            const double qg = c.rg_eq_ra ? qa : div_rn(r, c.rg, c.inv_rg);
+            const double qg = c.rg_eq_ra ? qa : div_rs(r, c.rg, c.inv_rg);
             const double w = RATIO ? ratio * s_wg(c, qg) : s_wg(c, qg);
-            g0 += div_rn(x[0] * w, c.r2g, c.inv_r2g) * c.rg;
-            g1 += div_rn(x[1] * w, c.r2g, c.inv_r2g) * c.rg;
-            g2 += div_rn(x[2] * w, c.r2g, c.inv_r2g) * c.rg;
+            g0 += div_rs(x[0] * w, c.r2g, c.inv_r2g) * c.rg;
+            g1 += div_rs(x[1] * w, c.r2g, c.inv_r2g) * c.rg;
+            g2 += div_rs(x[2] * w, c.r2g, c.inv_r2g) * c.rg;
         }
         if (in_p) {
-            const double qp = div_rn(r, c.rp, c.inv_rp);
+            const double qp = div_rs(r, c.rp, c.inv_rp);
             sum_p += s_wp(c, qp);
             const double dw = s_dwp(c, qp);
             const double ri = __drcp_rn(r);
-            const double e0 = div_rn(x[0], r, ri), e1 = div_rn(x[1], r, ri), e2 = div_rn(x[2], r, ri);
+            const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
             const double4 vj = vel[j];
             const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
             sum_d -= u0 * e0 * dw;
@@ -258,9 +268,9 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-        if (!(c.ra2 - r2 >= 0)) continue;
+        if (!(r2 <= c.ra2)) continue;
         const double r = sqrt(r2);
-        const double qa = div_rn(r, c.ra, c.inv_ra);
+        const double qa = div_rs(r, c.ra, c.inv_ra);
         sum_a += RATIO ? c.ratio[ti][type_of(pj)] * s_wa(c, qa) : s_wa(c, qa);
     }
     dens_a[i] = sum_a;
@@ -320,24 +330,25 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         // Without surface tension every CofA is 0, PressureA is +-0 and each
         // PressureA term adds a signed zero to a sum that starts at +0: the sum
         // stays +0 exactly, so the term is skipped (ST == false).
-        const bool in_p = c.rp2 - r2 > 0;
-        const bool in_a = !LRN && ST && (c.ra2 - r2 > 0);
-        const bool in_g = !LRN && ST && (c.rg2 - r2 > 0);
-        const bool in_v = !LRN && c.rv2 - r2 > 0;
+        // R*R - r2 > 0 (main.cpp:1926 and the other force sums) is r2 < R*R
+        const bool in_p = r2 < c.rp2;
+        const bool in_a = !LRN && ST && (r2 < c.ra2);
+        const bool in_g = !LRN && ST && (r2 < c.rg2);
+        const bool in_v = !LRN && r2 < c.rv2;
         if (!(in_p || in_a || in_g || in_v)) continue;
         const int tj = type_of(pj);
         const double r = sqrt(r2);
         const double ri = __drcp_rn(r);
-        const double e0 = div_rn(x[0], r, ri), e1 = div_rn(x[1], r, ri), e2 = div_rn(x[2], r, ri);
-        const double qa = div_rn(r, c.ra, c.inv_ra);
+        const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
+        const double qa = div_rs(r, c.ra, c.inv_ra);
         double rij = 1.0, rji = 1.0;
         if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
         const double4 vj = velp[j];   // .w = PressureP of j
         if (in_p) {
-            const double qp = div_rn(r, c.rp, c.inv_rp);
+            const double qp = div_rs(r, c.rp, c.inv_rp);
             const double dw = s_dwp(c, qp);
-            const double gw0 = div_rn(dw * x[0], r, ri), gw1 = div_rn(dw * x[1], r, ri),
-                         gw2 = div_rn(dw * x[2], r, ri);
+            const double gw0 = div_rs(dw * x[0], r, ri), gw1 = div_rs(dw * x[1], r, ri),
+                         gw2 = div_rs(dw * x[2], r, ri);
             const double ps = vi.w + vj.w;
             fp0 += ps * gw0 * c.vol;
             fp1 += ps * gw1 * c.vol;
@@ -355,13 +366,13 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         if (ST && in_g) {
             const double4 gcj = gcpa[j];
             const double aj = ai;
-            const double qg = c.rg_eq_ra ? qa : div_rn(r, c.rg, c.inv_rg);
+            const double qg = c.rg_eq_ra ? qa : div_rs(r, c.rg, c.inv_rg);
             const double wg = s_wg(c, qg);
             const double wij = RATIO ? rij * wg : wg;
             const double wji = RATIO ? rji * wg : wg;
-            fd0 -= div_rn(aj * gcj.x * wji - ai * gci.x * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
-            fd1 -= div_rn(aj * gcj.y * wji - ai * gci.y * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
-            fd2 -= div_rn(aj * gcj.z * wji - ai * gci.z * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd0 -= div_rs(aj * gcj.x * wji - ai * gci.x * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd1 -= div_rs(aj * gcj.y * wji - ai * gci.y * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd2 -= div_rs(aj * gcj.z * wji - ai * gci.z * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
             const double dg = s_dwg(c, qg);
             const double dwij = RATIO ? rij * dg : dg;
             const double dwji = RATIO ? rji * dg : dg;
@@ -369,19 +380,19 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
             gr += (aj * gcj.x * dwji - ai * gci.x * dwij) * x[0];
             gr += (aj * gcj.y * dwji - ai * gci.y * dwij) * x[1];
             gr += (aj * gcj.z * dwji - ai * gci.z * dwij) * x[2];
-            fd0 -= div_rn((gr) * e0, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
-            fd1 -= div_rn((gr) * e1, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
-            fd2 -= div_rn((gr) * e2, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd0 -= div_rs((gr) * e0, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd1 -= div_rs((gr) * e1, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+            fd2 -= div_rs((gr) * e2, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
         }
         if (in_v) {
-            const double qv = c.rv_eq_ra ? qa : div_rn(r, c.rv, c.inv_rv);
+            const double qv = c.rv_eq_ra ? qa : div_rs(r, c.rv, c.inv_rv);
             const double dw = -s_dwv(c, qv);
             const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
             const double cm = c.visc_mu[ti][tj];
             const double dot = u0 * e0 + u1 * e1 + u2 * e2;
-            fv0 += div_rn(cm * dot * e0 * dw, r, ri) * c.vol;
-            fv1 += div_rn(cm * dot * e1 * dw, r, ri) * c.vol;
-            fv2 += div_rn(cm * dot * e2 * dw, r, ri) * c.vol;
+            fv0 += div_rs(cm * dot * e0 * dw, r, ri) * c.vol;
+            fv1 += div_rs(cm * dot * e1 * dw, r, ri) * c.vol;
+            fv2 += div_rs(cm * dot * e2 * dw, r, ri) * c.vol;
         }
     }
     if (LRN) {

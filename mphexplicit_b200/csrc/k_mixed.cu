@@ -634,6 +634,75 @@ __global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, cons
     dens_a_out[i] = sa - ck;
 }
 
+// Virial pressure at particles for the mixed forms (output only; the FP64
+// form's k_virial restates main.cpp:2057-2302).  Only the trace of the pair
+// stress enters VirialPressureAtParticle = -trace / D, so each term reduces to
+// a scalar per pair (x = x_j - x_i, r = |x|, e = x / r):
+//   PressureP  (r < RP): P_i dwpdr(r) r
+//   PressureA  (r < RA): PA_i ratio_ij dwadr(r) r
+//   ViscosityV (r < RV): 0.5 C mu_ij (u_ij . e) (-dwvdr(r))
+//   DiffuseInterface (r < RG): a_i (GC_i . x) ratio_ij (wg + dwgdr r) Rg / R2g / l0
+// in FP32 on the exact cell-relative displacement, Kahan-compensated, with
+// the velocities after the step (the reference calls it after
+// calculateAcceleration, main.cpp:432-435).
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(128)
+k_mix_virial(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ pv,
+             const float4* __restrict__ gca, const double4* __restrict__ vel, const unsigned* __restrict__ list,
+             const int* __restrict__ cnt_short, const int* __restrict__ cnt_all, double* __restrict__ virial) {
+    __shared__ SharedTables tb;
+    load_tables(m, tb);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.n) return;
+    const float4 pi = phl[2 * (size_t)i];
+    const float4 li = phl[2 * (size_t)i + 1];
+    const int ti = __float_as_int(pi.w);
+    const float ppi = pv[2 * (size_t)i + 1].w;
+    const float4 gi = ST ? gca[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const double4 vd = vel[i];
+    const float vix = (float)vd.x, viy = (float)vd.y, viz = (float)vd.z;
+    const float ai = m.a_k[ti];
+    const float inv_l0 = 1.0f / m.l0;
+    const size_t n = (size_t)m.n;
+    float tr = 0.f, ck = 0.f;
+    auto visit = [&](unsigned e) {
+        const int j = (int)(e >> kCodeBits), code = (int)(e & 31u);
+        const float4 pj = phl[2 * (size_t)j];
+        const float4 lj = phl[2 * (size_t)j + 1];
+        const float4 dh = tb.dhi[code], dl = tb.dlo[code];
+        const float dx = ((pj.x - pi.x) + dh.x) + ((lj.x - li.x) + dl.x);
+        const float dy = ((pj.y - pi.y) + dh.y) + ((lj.y - li.y) + dl.y);
+        const float dz = ((pj.z - pi.z) + dh.z) + ((lj.z - li.z) + dl.z);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < m.rv2 || r2 < m.rp2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) return;
+        const float r = sqrtf(r2);
+        const int tj = __float_as_int(pj.w);
+        const float ratio = RATIO ? m.ratio[ti][tj] : 1.0f;
+        float t = 0.f;
+        if (r2 < m.rp2) t += ppi * (m.cp_m2 * (1.0f - r * m.inv_rp)) * r;
+        if (ST && r2 < m.ra2) {
+            const float q = r * m.inv_ra;
+            t += gi.w * ratio * (m.ca_inv * (1.0f - q) * (1.0f - 3.0f * q)) * r;
+        }
+        if (r2 < m.rv2) {
+            const double4 vj = vel[j];
+            const float ue = (((float)vj.x - vix) * dx + ((float)vj.y - viy) * dy + ((float)vj.z - viz) * dz) / r;
+            t += 0.5f * tb.mu[ti * 4 + tj] * ue * (-(m.cv_m2 * (1.0f - r * m.inv_rv)));
+        }
+        if (ST && r2 < m.rg2) {
+            const float q = 1.0f - r * m.inv_rg;
+            const float gx = gi.x * dx + gi.y * dy + gi.z * dz;
+            t += ai * gx * ratio * (m.cg * q * q + m.cg_m2 * q * r) * m.inv_r2g_rg * inv_l0;
+        }
+        kahan_add(tr, ck, t);
+    };
+    const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
+    const int ns = cnt_short[i], na = cnt_all[i];
+    for_entries(tab, n, ns, visit);
+    for_entries(tab + (size_t)(m.cap_s >> 2) * n, n, na - ns, visit);
+    virial[i] = -((double)tr - (double)ck) / (double)m.dim;
+}
+
 // NeighborCount for output: the list counts plus self (the reference lists
 // self), except walls without a fluid neighbour, whose list is empty there
 // (main.cpp:1416).
@@ -954,6 +1023,21 @@ int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, s
         m->exported = true;
     }
     if (launches) *launches = nl;
+    return MPH_OK;
+}
+
+int mixed_virial(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err) {
+    const int nb = blocks(c.n, 128);
+#define MIX_V(ST, RATIO)                                                                                    \
+    k_mix_virial<ST, RATIO><<<nb, 128, 0, s>>>(m->mc, m->phl, m->pv, m->gca, d.vel[d.vcur], m->list,        \
+                                               m->cnt_short, m->cnt_all, d.virial_p)
+    if (m->mc.has_st) {
+        if (m->mc.ratio_all_one) { MIX_V(true, false); } else { MIX_V(true, true); }
+    } else {
+        if (m->mc.ratio_all_one) { MIX_V(false, false); } else { MIX_V(false, true); }
+    }
+#undef MIX_V
+    MTRY(cudaGetLastError());
     return MPH_OK;
 }
 

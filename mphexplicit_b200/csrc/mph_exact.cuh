@@ -27,4 +27,20 @@ __device__ __forceinline__ double div_rn(double x, double y, double yi) {
     return x == 0.0 ? x * yi : q;
 }
 
+// div_rn without the zero-numerator branch, for the pair sweeps.  For x = +-0
+// the two corrections give +0 where x/y is -0 (x*yi gives the IEEE sign);
+// every quotient taken this way in the sweeps reaches the particle's state
+// only through products and sums that start at +0.0 (a DensityA / DensityP /
+// DivergenceP / GravityCenter / force accumulator), and such a sum never
+// holds -0.0 (+0 + -0 = +0, and an exact cancellation rounds to +0), so
+// adding a zero of either sign leaves it unchanged: the results are
+// bit-identical to those of div_rn (and of the reference's `/`).
+__device__ __forceinline__ double div_rs(double x, double y, double yi) {
+    double q = x * yi;
+    double r = __fma_rn(-q, y, x);
+    q = __fma_rn(r, yi, q);
+    r = __fma_rn(-q, y, x);
+    return __fma_rn(r, yi, q);
+}
+
 }  // namespace mph

@@ -267,6 +267,10 @@ int mph::make_simconst(const mph_params& p, const mph_grid_header& h, const mph_
         s.dmin[d] = h.domain_min[d];
         s.width[d] = c.domain_width[d];
         s.half_width[d] = 0.5 * c.domain_width[d];
+        {
+            const double q = 0.75 * c.domain_width[d];
+            std::memcpy(&s.q75_bits[d], &q, sizeof(q));
+        }
         s.cell_width[d] = c.cell_width[d];
     }
     if (s.cc[0] < 1 || s.cc[1] < 1 || s.cc[2] < 1 || s.tot < 1)
@@ -360,7 +364,7 @@ static int dalloc(mph_ctx* ctx, T** ptr, size_t count) {
 
 static void free_fp64(mph::DevFP64& d) {
     void* ptrs[] = {d.pidx[0], d.pidx[1], d.type[0], d.type[1], d.pos[0], d.pos[1], d.vel[0], d.vel[1],
-                    d.snap, d.force, d.dens_a, d.strain_p, d.div_p, d.press, d.gc, d.virial_p, d.keys,
+                    d.snap, d.pos32, d.force, d.dens_a, d.strain_p, d.div_p, d.press, d.gc, d.virial_p, d.keys,
                     d.vals, d.cellstart, d.ncount, d.nlist, d.ncount_s, d.nlist_s, d.wall_center, d.staging,
                     d.scal};
     for (void* q : ptrs)
@@ -384,6 +388,7 @@ static int alloc_fp64(mph_ctx* ctx) {
         TRY(dalloc(ctx, &d.vel[k], n));
     }
     TRY(dalloc(ctx, &d.snap, n));
+    TRY(dalloc(ctx, &d.pos32, n));
     TRY(dalloc(ctx, &d.force, n));
     TRY(dalloc(ctx, &d.dens_a, n));
     TRY(dalloc(ctx, &d.strain_p, n));
@@ -460,8 +465,10 @@ static int rebuild_fp64(mph_ctx* ctx) {
         CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_short, 0, sizeof(int), st));
         {
             Launch L(ctx, "neighbor_list");
-            mph::launch_neighbor_list(s, d.pos[d.cur], d.keys, d.cellstart, d.ncount, d.nlist, d.cap,
+            mph::launch_pos32(s, d.pos[d.cur], d.pos32, st);
+            mph::launch_neighbor_list(s, d.pos[d.cur], d.pos32, d.keys, d.cellstart, d.ncount, d.nlist, d.cap,
                                       sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.cap_s, d.scal, st);
+            L.count = 2;
         }
         CUDA_TRY(ctx, cudaGetLastError());
         CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_scal, d.scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, st));
@@ -1095,8 +1102,18 @@ extern "C" int mph_get_neighbors(mph_ctx* ctx, long long* ptr, int* ind, long lo
 
 extern "C" int mph_compute_virial(mph_ctx* ctx) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    if (ctx->mixed) return fail(ctx, MPH_ERR_STATE, "virial stress is computed by the FP64 form");
     mph::DevFP64& d = ctx->d;
+    if (ctx->mixed) {  // FP32 pair terms over the mixed form's own table (output only)
+        TRY(sync_state(ctx));
+        {
+            Launch L(ctx, "mix_virial");
+            const int rc = mph::mixed_virial(ctx->mixed, ctx->sc, d, ctx->stream, &ctx->err);
+            if (rc != MPH_OK) return fail(ctx, rc, ctx->err);
+        }
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        ctx->virial_valid = true;
+        return MPH_OK;
+    }
     ensure_density_a(ctx);  // the virial reads PressureA
     {
         Launch L(ctx, "virial");

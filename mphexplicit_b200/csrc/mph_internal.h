@@ -25,6 +25,10 @@ struct SimConst {
     int has_st;            // any surface tension -> diffuse-interface terms
     int ratio_all_one;     // InteractionRatio == 1 everywhere
     double dmin[3], width[3], half_width[3], cell_width[3];
+    // bits of 0.75*width: Mod(x, w) needs no division when 0 <= x < 0.75 w,
+    // tested as one unsigned compare of x's bit pattern (negative x, -0.0
+    // and NaN have the sign bit set and compare above every positive bound)
+    unsigned long long q75_bits[3];
     double dt, l0, vol, vol_over_l0;
     double n0a, n0p, r2g, cof_k;
     double ra, rg, rp, rv;             // radii
@@ -74,6 +78,7 @@ struct DevFP64 {
     int cur = 0;                            // index of the current pos/type/pidx
     int vcur = 0;                           // index of the current velocity
     double4* snap = nullptr;                // NeighborCalculatedPosition
+    float4* pos32 = nullptr;                // FP32 x - dmin for the list build's prefilter
     double4* force = nullptr;
     double* dens_a = nullptr;
     double* strain_p = nullptr;
@@ -103,9 +108,21 @@ void launch_cell_ranges(const SimConst& c, const int* keys, int* cellstart, cuda
 void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, const int* type_in,
                     const double4* pos_in, const double4* vel_in, int* pidx_out, int* type_out,
                     double4* pos_out, double4* vel_out, double4* snap, cudaStream_t s);
+// FP32 prefilter of the neighbour-list build: per axis whether it takes part,
+// the domain width, and the FP32 distance squared above which no candidate
+// can pass the exact FP64 test.
+struct Prefilter {
+    int use[3];
+    float width[3];
+    float r2_hi;
+};
+Prefilter make_prefilter(const SimConst& c);
+// FP32 positions relative to the domain origin (the prefilter's input).
+void launch_pos32(const SimConst& c, const double4* pos, float4* pos32, cudaStream_t s);
 // nlist_s != nullptr: also the short sublist (entries within rs2, in list
-// order; its longest length in scal->max_short).
-void launch_neighbor_list(const SimConst& c, const double4* pos, const int* keys,
+// order; its longest length in scal->max_short).  pos32 != nullptr: the FP32
+// prefilter skips candidates surely beyond the cut-off (same list).
+void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* keys,
                           const int* cellstart, int* ncount, int* nlist, int cap,
                           int* ncount_s, int* nlist_s, int cap_s, StepScalars* scal, cudaStream_t s);
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);

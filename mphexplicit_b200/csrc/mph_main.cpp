@@ -152,10 +152,8 @@ int main(int argc, char** argv) {
         ++steps;
         if (Time + 1.0e-5 * Dt >= VtkOutputNext) {
             const auto b = clk::now();
-            if (mode == MPH_MODE_FP64) {
-                st = mph_compute_virial(ctx);
-                if (st != MPH_OK) return die(ctx, st, "virial");
-            }
+            st = mph_compute_virial(ctx);  // every form: VirialPressureAtParticle is a VTK field
+            if (st != MPH_OK) return die(ctx, st, "virial");
             std::snprintf(fname, sizeof(fname), vtk.c_str(), iStep);
             st = mph_write_vtk_async(ctx, fname);
             if (st != MPH_OK) return die(ctx, st, "writing a vtk file");

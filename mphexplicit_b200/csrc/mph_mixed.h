@@ -27,6 +27,8 @@ void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wa
 int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
 // Fill the output-only fields (DensityA, wall forces, neighbour counts).
 int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);
+// VirialPressureAtParticle into d.virial_p (FP32 pair terms, output only).
+int mixed_virial(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err);
 // Positions/velocities were overwritten in `d` (mph_set_state): refresh.
 int mixed_import(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err);
 void mixed_mark_stale(MixedState* m);

@@ -61,6 +61,33 @@ def test_noalloc_cell_sort_matches_existing_path_twice():
         assert np.array_equal(cs[tot + 1:2 * tot + 1], cells["wall_end"])
 
 
+def test_noalloc_call_allocates_no_device_memory():
+    """After a first call on the device (its set-up), further calls change
+    neither the device's free memory nor torch's allocations."""
+    import torch
+    stream = torch.cuda.Stream()
+    sc = scenes.dam_break_3d(fluid=(10, 8, 12), box=(24, 8, 18), walls=3, seed=43)
+    first = _noalloc_sort(sc, stream)
+    lib = N.load()
+    c = M.compute_constants(sc.params, sc.header, sc.dim)
+    tot = c.total_cell_count
+    xyz = torch.tensor(np.ascontiguousarray(sc.xyz), dtype=torch.float64, device="cuda")
+    typ = torch.tensor(sc.type, dtype=torch.int32, device="cuda")
+    out = [torch.zeros(k, dtype=torch.int32, device="cuda") for k in (sc.n, sc.n, 2 * tot + 1)]
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    alloc1 = torch.cuda.memory_allocated()
+    for _ in range(3):
+        st = lib.mph_cell_sort_noalloc(C.byref(c), C.byref(sc.header), sc.n, _ptr(xyz), _ptr(typ), _ptr(out[0]),
+                                       _ptr(out[1]), _ptr(out[2]), C.c_void_p(stream.cuda_stream))
+        assert st == 0, st
+    stream.synchronize()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free1
+    assert torch.cuda.memory_allocated() == alloc1
+    assert np.array_equal(out[0].cpu().numpy(), first[1]) and np.array_equal(out[1].cpu().numpy(), first[2])
+
+
 def test_noalloc_cell_sort_rejects_oversize():
     import torch
     sc = scenes.droplet_2d(n=8)
