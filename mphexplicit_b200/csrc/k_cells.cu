@@ -178,9 +178,12 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
     for (int d = 0; d < 3; ++d) {
         const int r = c.range[d];
         w[d] = 2 * r + 1;
+        // a wall's key carries +TotalCellCount, so its icx is cx + cc[0]: the
+        // image offset is taken from the home cell reduced into [0, cc)
+        const int home = ic[d] % c.cc[d];
         for (int j = 0; j < w[d]; ++j) {
-            const int raw = ic[d] - r + j;
-            jc[d][j] = (raw % c.cc[d] + c.cc[d]) % c.cc[d];
+            jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
+            const int raw = home - r + j;
             jo[d][j] = raw < 0 ? -pf.width[d] : (raw >= c.cc[d] ? pf.width[d] : 0.0f);
         }
         const int b = (2 * r) - (ic[d] + r) % c.cc[d];       // main.cpp:1376-1381
