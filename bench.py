@@ -194,7 +194,11 @@ def measure_learned(args, rank):
     t0 = time.perf_counter()
     m = LR.Model(seed=rank)
     m.fit_scales(ds)
-    loss = m.train(ds, epochs=args.learn_epochs, batch=4096, lr=2e-3, seed=rank)
+    # Adam in three phases of falling step size (2e-3, 6e-4, 2e-4)
+    loss = None
+    per_phase = max(1, args.learn_epochs // 3)
+    for k, lr in enumerate((2e-3, 6e-4, 2e-4)):
+        loss = m.train(ds, epochs=per_phase, batch=4096, lr=lr, seed=rank * 7 + k)
     t_train = time.perf_counter() - t0
     n_samples = len(ds)
     ds.close()
@@ -232,7 +236,8 @@ def measure_learned(args, rank):
            "judge_interval": 20, "tolerance": 1e-2,
            "fallback_rate": stats["plain_steps"] / max(1, stats["steps"]), "judge": stats,
            "kernels_ms_per_step": {k: v[1] / steps for k, v in prof.items()},
-           "training": {"fp64_steps": seeds * per, "seeds": seeds, "samples": n_samples, "epochs": args.learn_epochs,
+           "training": {"fp64_steps": seeds * per, "seeds": seeds, "samples": n_samples, "epochs": 3 * per_phase,
+                        "learning_rates": [2e-3, 6e-4, 2e-4],
                         "final_loss": loss, "data_s": t_data, "train_s": t_train}}
     if "mlp_edges" in prof:
         nl, tot = prof["mlp_edges"]
@@ -641,7 +646,7 @@ def main():
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
-    ap.add_argument("--learn-epochs", type=int, default=4)
+    ap.add_argument("--learn-epochs", type=int, default=30)
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--output-every", type=int, default=100, help="steps between VTK files written behind the step")
     ap.add_argument("--output-files", type=int, default=5)
