@@ -18,13 +18,14 @@
 
 // Resident 128-thread blocks per SM the sweeps are compiled for (register cap
 // 65536 / (128 * blocks)); latency hiding vs. spills, set by measurement on
-// the full dam break: sweep A 8 (64 registers), the force sweep 7 (73
-// registers, no spills; 7 % faster than at 8).
+// the full dam break: sweep A 8 (64 registers); the force sweep, which keeps
+// the next neighbour's records in flight, 5 (94 registers, no spills: 3.46 ms
+// against 3.69 ms without the prefetch at 7 blocks, 4.21 ms with it at 6).
 #ifndef MPH_SWEEP_MINB
 #define MPH_SWEEP_MINB 8
 #endif
 #ifndef MPH_SWEEPB_MINB
-#define MPH_SWEEPB_MINB 7
+#define MPH_SWEEPB_MINB 5
 #endif
 
 namespace mph {
@@ -316,14 +317,26 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     double fa0 = 0.0, fa1 = 0.0, fa2 = 0.0;
     double fd0 = 0.0, fd1 = 0.0, fd2 = 0.0;
     double fv0 = 0.0, fv1 = 0.0, fv2 = 0.0;
+    // software pipeline: list indices two entries ahead, the neighbour's two
+    // records (position, velocity + PressureP) one entry ahead, so their
+    // gathers overlap the previous pair's FP64 arithmetic
     const int* lp = nlist + i;
-    int jn = cnt > 0 ? __ldg(lp) : 0;  // next index, loaded one iteration ahead
+    int j1 = cnt > 0 ? __ldg(lp) : i;
+    int j2 = cnt > 1 ? __ldg(lp + n) : i;
+    lp += 2 * n;
+    double4 pn = pos[j1], vn1 = velp[j1];
     for (int k = 0; k < cnt; ++k) {
-        const int j = jn;
+        const int j = j1;
+        const double4 pj = pn;
+        const double4 vj = vn1;   // .w = PressureP of j
+        j1 = j2;
+        if (k + 2 < cnt) j2 = __ldg(lp);
         lp += n;
-        if (k + 1 < cnt) jn = __ldg(lp);
+        if (k + 1 < cnt) {
+            pn = pos[j1];
+            vn1 = velp[j1];
+        }
         if (j == i) continue;
-        const double4 pj = pos[j];
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
@@ -343,7 +356,6 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         const double qa = div_rs(r, c.ra, c.inv_ra);
         double rij = 1.0, rji = 1.0;
         if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
-        const double4 vj = velp[j];   // .w = PressureP of j
         if (in_p) {
             const double qp = div_rs(r, c.rp, c.inv_rp);
             const double dw = s_dwp(c, qp);

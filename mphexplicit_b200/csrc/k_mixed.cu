@@ -51,6 +51,7 @@ struct MixConst {
     float v_a, v_b;                    // viscosity: -cv*(-2/rv)*vol * (1 - r/rv) = v_a + v_b*r
     float vol, vol_over_l0, n0a, n0p, inv_r2g_rg, l0;
     double p_a_d, p_b_d, v_a_d, v_b_d, cp_d, cp_m2_d, inv_rp_d, n0p_d;  // FP64 pressure core
+    float inv_rp_lo, cp_lo;            // 1/RP and Cp as FP32 pairs: (inv_rp, inv_rp_lo), (cp, cp_lo)
     float visc_mu[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
     float ratio[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
     float a_k[MPH_TYPE_COUNT], cof_a[MPH_TYPE_COUNT];
@@ -361,6 +362,53 @@ __device__ __forceinline__ void load_tables(const MixConst& m, SharedTables& t) 
     __syncthreads();
 }
 
+// One DensityP term wp = Cp (1 - r/RP)^2 as an unevaluated sum of two FP32
+// numbers, added to the pair sum (sh, sl), with FP32 operations only.  The
+// displacement arrives as its exact hi part (grid multiples) and its small lo
+// part; error-free transformations (Knuth's TwoSum, Dekker's Fast2Sum, the
+// FMA product error a*b - RN(a*b); Muller et al., Handbook of Floating-Point
+// Arithmetic, chs. 4-5) carry r^2, r, 1 - r/RP and the square to about 2^-44
+// relative.  The strain is a small difference of a sum near N0p, so the
+// per-term rounding of plain FP32 (~1e-7 relative) would dominate the error.
+__device__ __forceinline__ void wp_df(const MixConst& m, float hx, float hy, float hz, float lx, float ly,
+                                      float lz, float& sh, float& sl) {
+    // renormalise each axis so that hi is the FP32 rounding of hi + lo
+    { const float t = hx + lx; lx -= t - hx; hx = t; }
+    { const float t = hy + ly; ly -= t - hy; hy = t; }
+    { const float t = hz + lz; lz -= t - hz; hz = t; }
+    const float px = hx * hx, py = hy * hy, pz = hz * hz;
+    const float ex = fmaf(hx, hx, -px), ey = fmaf(hy, hy, -py), ez = fmaf(hz, hz, -pz);
+    const float s1 = px + py;
+    float bb = s1 - px;
+    const float e1 = (px - (s1 - bb)) + (py - bb);
+    const float s2 = s1 + pz;
+    bb = s2 - s1;
+    const float e2 = (s1 - (s2 - bb)) + (pz - bb);
+    float lo = e1 + e2 + ex + ey + ez + 2.0f * (hx * lx + hy * ly + hz * lz);
+    const float hi = s2 + lo;
+    lo -= hi - s2;
+    // r = sqrt(hi + lo): r0 + rl
+    const float y = rsqrt_nr(hi);
+    const float r0 = hi * y;
+    const float rl = (fmaf(-r0, r0, hi) + lo) * (0.5f * y);
+    // q = 1 - r / RP: qh + ql
+    const float t = r0 * m.inv_rp;
+    const float te = fmaf(r0, m.inv_rp, -t) + r0 * m.inv_rp_lo + rl * m.inv_rp;
+    const float qh = 1.0f - t;
+    const float ql = ((1.0f - qh) - t) - te;
+    // w = Cp q^2: wh + wl
+    const float p2 = qh * qh;
+    const float p2e = fmaf(qh, qh, -p2) + 2.0f * qh * ql;
+    const float wh = m.cp * p2;
+    const float wl = fmaf(m.cp, p2, -wh) + m.cp * p2e + m.cp_lo * p2;
+    // (sh, sl) += (wh, wl)
+    const float sn = sh + wh;
+    bb = sn - sh;
+    const float se = (sh - (sn - bb)) + (wh - bb);
+    sh = sn;
+    sl += se + wl;
+}
+
 // Sweep A: DensityP and DivergenceP over the short part of the list with the
 // exact FP32 displacement (S64: pair arithmetic in FP64, the displacement
 // assembled in FP64 from the hi/lo parts, FP32 velocities), plus, with
@@ -389,7 +437,7 @@ k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v
     const int ns = cnt_short[i];
     const int na = ST ? cnt_all[i] : ns;
     const size_t n = (size_t)m.n;
-    float sp = 0.f, cpk = 0.f, sd = 0.f, cdk = 0.f;
+    float sph = 0.f, spl = 0.f, sd = 0.f, cdk = 0.f;
     double spd = 0.0, sdd = 0.0;
     float sa = 0.f, cak = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
     const uint4* tab = reinterpret_cast<const uint4*>(list) + i;
@@ -427,8 +475,9 @@ k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v
         const float rinv = rsqrt_nr(r2);
         const float r = r2 * rinv;
         if (!S64 && r2 <= m.rp2) {
+            wp_df(m, (pj.x - pi.x) + dh.x, (pj.y - pi.y) + dh.y, (pj.z - pi.z) + dh.z, (lj.x - li.x) + dl.x,
+                  (lj.y - li.y) + dl.y, (lj.z - li.z) + dl.z, sph, spl);  // wp
             const float q = 1.0f - r * m.inv_rp;
-            kahan_add(sp, cpk, m.cp * q * q);                   // wp
             const float dw = m.cp_m2 * q;                        // dwpdr
             const float4 vj = v32[j];
             const float ue = ((vj.x - vi.x) * dx + (vj.y - vi.y) * dy + (vj.z - vi.z) * dz) * rinv;
@@ -451,9 +500,9 @@ k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v
         strain = spd - m.n0p_d;
         div = sdd;
     } else {
-        // the compensated sum keeps its low part: N0p is subtracted in FP64
-        // (the strain is a small difference of two numbers near N0p)
-        strain = ((double)sp - (double)cpk) - m.n0p_d;
+        // the pair sum is exact to ~2^-44: N0p is subtracted in FP64 (the
+        // strain is a small difference of two numbers near N0p)
+        strain = ((double)sph + (double)spl) - m.n0p_d;
         div = (double)sd - (double)cdk;
     }
     double kappa = c.bulk_modulus[ti];
@@ -940,6 +989,8 @@ int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, De
     mc.cp_m2_d = c.cp * c.m2_rp;
     mc.inv_rp_d = 1.0 / c.rp;
     mc.n0p_d = c.n0p;
+    mc.inv_rp_lo = (float)(1.0 / c.rp - (double)mc.inv_rp);
+    mc.cp_lo = (float)(c.cp - (double)mc.cp);
     mc.vol = (float)c.vol;
     mc.vol_over_l0 = (float)c.vol_over_l0;
     mc.n0a = (float)c.n0a;
