@@ -143,102 +143,136 @@ __global__ void k_reorder(int n, const int* __restrict__ vals, const int* __rest
     vel_out[i] = vel_in[s];
 }
 
-// Neighbour list, one thread per particle (main.cpp:1329-1585).  The count and
-// the fill of the reference are one pass here: entries go to a column-major
-// [cap][n] table; a list longer than cap is still counted, raises
-// DEVFLAG_NEIGHBOR_OVERFLOW and the host rebuilds with a larger table.  With
-// nlist_s, the entries within rs2 also go, in the same order, to the short
-// sublist: a particle moves at most MARGIN/2 between builds (the rebuild test
-// of main.cpp:1086-1108), so every pair within RadiusP until the next build is
-// in it, and a sum over the pairs within RadiusP visits them in list order.
+// Neighbour list (main.cpp:1329-1585), one warp per home key: the particles
+// of one cell (fluid keys, then the wall keys of the same cells) share their
+// 3^D stencil and its visiting order, so the warp walks it in step, 32 home
+// particles at a time (one per lane).  Each candidate range is read 32
+// candidates at a time (one coalesced FP32 record per lane into shared
+// memory); every lane then tests all of them against its own particle with
+// the FP32 prefilter, giving a bit mask, and runs the exact FP64 test of the
+// reference only over the set bits, in ascending order.  A lane's entries
+// are therefore the reference's, in the reference's order: fluid candidates
+// of the 27 cells, then wall candidates (a wall with no fluid neighbour
+// skips the walls, main.cpp:1416), self included, each range ascending.
 //
-// Prefilter (pos32 != nullptr): FP32 positions relative to the domain origin
-// (k_pos32) give a displacement within the bound of make_prefilter of the one
-// the exact FP64 test computes, so a candidate whose FP32 distance squared
-// exceeds pf.r2_hi cannot pass that test and is skipped; every other candidate
-// takes the exact test.  The list is therefore the same, entry for entry.  An
-// axis with fewer than 4 cells contributes nothing to the FP32 distance (its
-// minimum image need not be the neighbouring cell's), which only keeps more
-// candidates.
-__global__ void __launch_bounds__(256)
+// The count and the fill of the reference are one pass: entries go to a
+// column-major [cap][n] table; a list longer than cap is still counted,
+// raises DEVFLAG_NEIGHBOR_OVERFLOW and the host rebuilds with a larger table.
+// With nlist_s, the entries within rs2 also go, in the same order, to the
+// short sublist: a particle moves at most MARGIN/2 between builds (the
+// rebuild test of main.cpp:1086-1108), so every pair within RadiusP until the
+// next build is in it, and a sum over the pairs within RadiusP visits them in
+// list order.
+//
+// Prefilter: FP32 positions relative to the domain origin (k_pos32) give a
+// displacement within the bound of make_prefilter of the one the exact FP64
+// test computes, so a candidate whose FP32 distance squared exceeds pf.r2_hi
+// cannot pass that test and is skipped.  An axis with fewer than 4 cells
+// contributes nothing to the FP32 distance (its minimum image need not be the
+// neighbouring cell's), which only keeps more candidates.
+constexpr int kListWarps = 4;  // warps (home keys) per 128-thread block
+
+__global__ void __launch_bounds__(32 * kListWarps, 6)
 k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __restrict__ pos32, Prefilter pf,
-                const int* __restrict__ keys, const int* __restrict__ cellstart, int* __restrict__ ncount,
-                int* __restrict__ nlist, int cap, int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s,
-                StepScalars* __restrict__ scal) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    const int ci = keys[i];
-    const int icx = (ci / (c.cc[1] * c.cc[2])) % c.tot;     // main.cpp:1356-1358
-    const int icy = (ci / c.cc[2]) % c.cc[1];
-    const int icz = ci % c.cc[2];
-    int jc[3][3];
-    float jo[3][3];  // FP32 image offset of each stencil slot (0, or -+ the domain width where it wraps)
-    const int ic[3] = {icx, icy, icz};
-    int jmin[3], w[3];
+                const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist, int cap,
+                int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s, StepScalars* __restrict__ scal) {
+    __shared__ float4 cand[kListWarps][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int key = blockIdx.x * kListWarps + wib;  // home key in [0, 2*tot)
+    if (key >= 2 * c.tot) return;                   // whole warp
+    const int hb = cellstart[key], he = cellstart[key + 1];
+    if (hb == he) return;
+    // the stencil of the home cell as main.cpp:1356-1392 computes it from the
+    // key (a wall's key carries +TotalCellCount: its icx is cx + cc[0])
+    const int icx = (key / (c.cc[1] * c.cc[2])) % c.tot;
+    const int ic[3] = {icx, (key / c.cc[2]) % c.cc[1], key % c.cc[2]};
+    int jmin[3], w[3], home[3];
     for (int d = 0; d < 3; ++d) {
         const int r = c.range[d];
         w[d] = 2 * r + 1;
-        // a wall's key carries +TotalCellCount, so its icx is cx + cc[0]: the
-        // image offset is taken from the home cell reduced into [0, cc)
-        const int home = ic[d] % c.cc[d];
-        for (int j = 0; j < w[d]; ++j) {
-            jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
-            const int raw = home - r + j;
-            jo[d][j] = raw < 0 ? -pf.width[d] : (raw >= c.cc[d] ? pf.width[d] : 0.0f);
-        }
-        const int b = (2 * r) - (ic[d] + r) % c.cc[d];       // main.cpp:1376-1381
+        home[d] = ic[d] % c.cc[d];
+        const int b = (2 * r) - (ic[d] + r) % c.cc[d];  // main.cpp:1376-1381
         jmin[d] = b > 0 ? b : 0;
     }
-    const double4 pi = pos[i];
-    const bool filter = pos32 != nullptr;
-    const float4 pf_i = filter ? pos32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // stencil slot s of axis d: the cell coordinate (main.cpp:1360-1372) and
+    // the FP32 image offset (0, or -+ the domain width where the slot wraps)
+    auto slot = [&](int d, int s_, float& off) {
+        const int raw = home[d] - c.range[d] + s_;
+        off = raw < 0 ? -pf.width[d] : (raw >= c.cc[d] ? pf.width[d] : 0.0f);
+        return ((ic[d] - c.range[d] + s_) % c.cc[d] + c.cc[d]) % c.cc[d];
+    };
     const int wall_begin = cellstart[c.tot], wall_end = cellstart[2 * c.tot];
     const size_t n = (size_t)c.n;
-    int cnt = 0, cnt_s = 0;
     const bool short_list = nlist_s != nullptr;
-    for (int kind = 0; kind < 2; ++kind) {
-        if (kind == 1 && wall_begin <= i && i < wall_end && cnt == 0) break;  // main.cpp:1416
-        const int off = kind ? c.tot : 0;
-        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
-                    const int sx = jx % w[0], sy = jy % w[1], sz = jz % w[2];
-                    const int cell = cell_id(c, jc[0][sx], jc[1][sy], jc[2][sz]);
-                    const float ox = pf.use[0] ? jo[0][sx] - pf_i.x : 0.f;
-                    const float oy = pf.use[1] ? jo[1][sy] - pf_i.y : 0.f;
-                    const float oz = pf.use[2] ? jo[2][sz] - pf_i.z : 0.f;
-                    const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
-                    for (int j = b; j < e; ++j) {
-                        if (filter) {
-                            const float4 q = pos32[j];
-                            const float fx = pf.use[0] ? q.x + ox : 0.f;
-                            const float fy = pf.use[1] ? q.y + oy : 0.f;
-                            const float fz = pf.use[2] ? q.z + oz : 0.f;
-                            if (fx * fx + fy * fy + fz * fz > pf.r2_hi) continue;
-                        }
-                        const double4 pj = pos[j];
-                        const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-                        const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-                        const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
-                        const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-                        if (r2 <= c.rm2) {
-                            if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
-                            cnt++;
-                            if (short_list && r2 <= c.rs2) {
-                                if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
-                                cnt_s++;
+    float4* cw = cand[wib];
+    for (int h0 = hb; h0 < he; h0 += 32) {
+        const int i = h0 + lane;
+        const bool active = i < he;
+        const double4 pi = pos[active ? i : hb];
+        const float4 fi = pos32[active ? i : hb];
+        const bool is_wall = wall_begin <= i && i < wall_end;
+        int cnt = 0, cnt_s = 0;
+        for (int kind = 0; kind < 2; ++kind) {
+            // main.cpp:1416: a wall with no fluid neighbour gets no wall entries
+            const bool take = active && !(kind == 1 && is_wall && cnt == 0);
+            const int off = kind ? c.tot : 0;
+            for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+                for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+                    for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                        float gx, gy, gz;
+                        const int cx = slot(0, jx % w[0], gx), cy = slot(1, jy % w[1], gy),
+                                  cz = slot(2, jz % w[2], gz);
+                        const int cell = cell_id(c, cx, cy, cz);
+                        const float ox = pf.use[0] ? gx - fi.x : 0.f;
+                        const float oy = pf.use[1] ? gy - fi.y : 0.f;
+                        const float oz = pf.use[2] ? gz - fi.z : 0.f;
+                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                        for (int cb = b; cb < e; cb += 32) {
+                            const int m = min(32, e - cb);
+                            __syncwarp();
+                            if (lane < m) cw[lane] = pos32[cb + lane];
+                            __syncwarp();
+                            unsigned mask = 0u;
+                            if (take) {
+                                for (int t = 0; t < m; ++t) {
+                                    const float4 q = cw[t];
+                                    const float fx = pf.use[0] ? q.x + ox : 0.f;
+                                    const float fy = pf.use[1] ? q.y + oy : 0.f;
+                                    const float fz = pf.use[2] ? q.z + oz : 0.f;
+                                    if (fx * fx + fy * fy + fz * fz <= pf.r2_hi) mask |= 1u << t;
+                                }
+                            }
+                            while (mask) {
+                                const int t = __ffs(mask) - 1;
+                                mask &= mask - 1u;
+                                const int j = cb + t;
+                                const double4 pj = pos[j];
+                                const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+                                const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+                                const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+                                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                                if (r2 <= c.rm2) {
+                                    if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
+                                    cnt++;
+                                    if (short_list && r2 <= c.rs2) {
+                                        if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
+                                        cnt_s++;
+                                    }
+                                }
                             }
                         }
                     }
-                }
-    }
-    ncount[i] = cnt;
-    atomicMax(&scal->max_neighbors, cnt);
-    if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
-    if (short_list) {
-        ncount_s[i] = cnt_s;
-        atomicMax(&scal->max_short, cnt_s);
-        if (cnt_s > cap_s) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+        }
+        if (active) {
+            ncount[i] = cnt;
+            atomicMax(&scal->max_neighbors, cnt);
+            if (cnt > cap) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+            if (short_list) {
+                ncount_s[i] = cnt_s;
+                atomicMax(&scal->max_short, cnt_s);
+                if (cnt_s > cap_s) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+            }
+        }
     }
 }
 
@@ -348,11 +382,12 @@ void launch_pos32(const SimConst& c, const double4* pos, float4* pos32, cudaStre
     k_pos32<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, pos32);
 }
 
-void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* keys,
-                          const int* cellstart, int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s,
-                          int cap_s, StepScalars* scal, cudaStream_t s) {
-    k_neighbor_list<<<blocks(c.n, 256), 256, 0, s>>>(c, pos, pos32, make_prefilter(c), keys, cellstart, ncount,
-                                                     nlist, cap, ncount_s, nlist_s, cap_s, scal);
+void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* cellstart,
+                          int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
+                          StepScalars* scal, cudaStream_t s) {
+    const long long keys = 2LL * c.tot;
+    k_neighbor_list<<<(int)((keys + kListWarps - 1) / kListWarps), 32 * kListWarps, 0, s>>>(
+        c, pos, pos32, make_prefilter(c), cellstart, ncount, nlist, cap, ncount_s, nlist_s, cap_s, scal);
 }
 
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s) {

@@ -197,83 +197,107 @@ __global__ void k_mix_home(SimConst c, MixConst m, const double4* __restrict__ p
     v32[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.0f);
 }
 
-// Neighbour table: for particle i, the 3^D stencil (same visiting order as
-// main.cpp:1356-1392), entries (j << 5 | code), in one pass: pairs within
+// Neighbour table, one warp per home key (the particles of one cell, fluid
+// keys then the wall keys of the same cells): the lanes share the 3^D stencil
+// (same visiting order as main.cpp:1356-1392) and walk it in step, 32 home
+// particles at a time.  Each candidate range is read 32 records at a time
+// (coalesced, into shared memory) and every lane tests all of them in FP32 on
+// the cell-relative hi parts.  Entries are (j << 5 | code): pairs within
 // RP+margin go to rows [0, cap_s), the rest within MaxRadius+margin to rows
 // [cap_s, cap_s + cap_l), each part in stencil order.  Self is excluded.
 // Walls without a fluid neighbour get no list (their pressure is never used).
-__global__ void __launch_bounds__(128)
-k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __restrict__ keys,
-           const int* __restrict__ cellstart, unsigned* __restrict__ list, int cap_l, int* __restrict__ cnt_short,
-           int* __restrict__ cnt_all, StepScalars* __restrict__ scal) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    int ci = keys[i];
-    if (ci >= c.tot) ci -= c.tot;
+constexpr int kMixListWarps = 4;
+
+__global__ void __launch_bounds__(32 * kMixListWarps, 6)
+k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __restrict__ cellstart,
+           unsigned* __restrict__ list, int cap_l, int* __restrict__ cnt_short, int* __restrict__ cnt_all,
+           StepScalars* __restrict__ scal) {
+    __shared__ float4 cand[kMixListWarps][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int key = blockIdx.x * kMixListWarps + wib;
+    if (key >= 2 * c.tot) return;  // whole warp
+    const int hb = cellstart[key], he = cellstart[key + 1];
+    if (hb == he) return;
+    const int ci = key >= c.tot ? key - c.tot : key;
     const int ic[3] = {ci / (c.cc[1] * c.cc[2]), (ci / c.cc[2]) % c.cc[1], ci % c.cc[2]};
-    int jc[3][3], jmin[3], w[3];
+    int jmin[3], w[3];
     for (int d = 0; d < 3; ++d) {
         const int r = c.range[d];
         w[d] = 2 * r + 1;
-        for (int j = 0; j < w[d]; ++j) jc[d][j] = ((ic[d] - r + j) % c.cc[d] + c.cc[d]) % c.cc[d];
         const int b = (2 * r) - (ic[d] + r) % c.cc[d];
         jmin[d] = b > 0 ? b : 0;
     }
-    const float4 pi = p32[i];
     const int nf = cellstart[c.tot];
-    const bool is_wall = i >= nf;
     const size_t n = (size_t)c.n;
     const int cap_s = m.cap_s;
-    uint4* const ls = reinterpret_cast<uint4*>(list) + i;
-    uint4* const ll = reinterpret_cast<uint4*>(list) + (size_t)(cap_s >> 2) * n + i;
-    int cs = 0, cl = 0;
-    unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, l0 = 0, l1 = 0, l2 = 0, l3 = 0;  // rows being filled
-    auto push = [n](unsigned e, int& cnt, int cap, uint4* row0, unsigned& b0, unsigned& b1, unsigned& b2,
-                    unsigned& b3) {
-        switch (cnt & 3) {
-            case 0: b0 = e; break;
-            case 1: b1 = e; break;
-            case 2: b2 = e; break;
-            default:
-                b3 = e;
-                if (cnt < cap) row0[(size_t)(cnt >> 2) * n] = make_uint4(b0, b1, b2, b3);
-        }
-        ++cnt;
-    };
-    bool any_fluid = !is_wall;  // a wall needs a list only if a fluid particle is within reach
-    for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-        for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-            for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
-                const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
-                const int cell = jc[0][ax] * c.cc[1] * c.cc[2] + jc[1][ay] * c.cc[2] + jc[2][az];
-                const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
-                const float ox = m.dhi[code][0], oy = m.dhi[code][1], oz = m.dhi[code][2];
-                for (int kind = 0; kind < 2; ++kind) {
-                    const int off = kind ? c.tot : 0;
-                    const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
-                    for (int j = b; j < e; ++j) {
-                        if (j == i) continue;
-                        const float4 pj = p32[j];
-                        const float dx = (pj.x - pi.x) + ox, dy = (pj.y - pi.y) + oy, dz = (pj.z - pi.z) + oz;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        if (r2 < m.list_r2) {
-                            if (kind == 0) any_fluid = true;
-                            const unsigned entry = ((unsigned)j << kCodeBits) | (unsigned)code;
-                            if (r2 < m.short_r2) push(entry, cs, cap_s, ls, s0, s1, s2, s3);
-                            else push(entry, cl, cap_l, ll, l0, l1, l2, l3);
+    float4* cw = cand[wib];
+    for (int h0 = hb; h0 < he; h0 += 32) {
+        const int i = h0 + lane;
+        const bool active = i < he;
+        const float4 pi = p32[active ? i : hb];
+        const bool is_wall = i >= nf;
+        uint4* const ls = reinterpret_cast<uint4*>(list) + i;
+        uint4* const ll = reinterpret_cast<uint4*>(list) + (size_t)(cap_s >> 2) * n + i;
+        int cs = 0, cl = 0;
+        unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, l0 = 0, l1 = 0, l2 = 0, l3 = 0;  // rows being filled
+        auto push = [n](unsigned e, int& cnt, int cap, uint4* row0, unsigned& b0, unsigned& b1, unsigned& b2,
+                        unsigned& b3) {
+            switch (cnt & 3) {
+                case 0: b0 = e; break;
+                case 1: b1 = e; break;
+                case 2: b2 = e; break;
+                default:
+                    b3 = e;
+                    if (cnt < cap) row0[(size_t)(cnt >> 2) * n] = make_uint4(b0, b1, b2, b3);
+            }
+            ++cnt;
+        };
+        bool any_fluid = !is_wall;  // a wall needs a list only if a fluid particle is within reach
+        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                    const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
+                    const int cx = ((ic[0] - c.range[0] + ax) % c.cc[0] + c.cc[0]) % c.cc[0];
+                    const int cy = ((ic[1] - c.range[1] + ay) % c.cc[1] + c.cc[1]) % c.cc[1];
+                    const int cz = ((ic[2] - c.range[2] + az) % c.cc[2] + c.cc[2]) % c.cc[2];
+                    const int cell = cx * c.cc[1] * c.cc[2] + cy * c.cc[2] + cz;
+                    const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
+                    const float ox = m.dhi[code][0] - pi.x, oy = m.dhi[code][1] - pi.y, oz = m.dhi[code][2] - pi.z;
+                    for (int kind = 0; kind < 2; ++kind) {
+                        const int off = kind ? c.tot : 0;
+                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                        for (int cb = b; cb < e; cb += 32) {
+                            const int mm = min(32, e - cb);
+                            __syncwarp();
+                            if (lane < mm) cw[lane] = p32[cb + lane];
+                            __syncwarp();
+                            if (!active) continue;
+                            for (int t = 0; t < mm; ++t) {
+                                const int j = cb + t;
+                                const float4 q = cw[t];
+                                const float dx = q.x + ox, dy = q.y + oy, dz = q.z + oz;
+                                const float r2 = dx * dx + dy * dy + dz * dz;
+                                if (r2 < m.list_r2 && j != i) {
+                                    if (kind == 0) any_fluid = true;
+                                    const unsigned entry = ((unsigned)j << kCodeBits) | (unsigned)code;
+                                    if (r2 < m.short_r2) push(entry, cs, cap_s, ls, s0, s1, s2, s3);
+                                    else push(entry, cl, cap_l, ll, l0, l1, l2, l3);
+                                }
+                            }
                         }
                     }
                 }
-            }
-    if ((cs & 3) != 0 && cs < cap_s) ls[(size_t)(cs >> 2) * n] = make_uint4(s0, s1, s2, s3);
-    if ((cl & 3) != 0 && cl < cap_l) ll[(size_t)(cl >> 2) * n] = make_uint4(l0, l1, l2, l3);
-    if (is_wall && !any_fluid) cs = cl = 0;
-    cnt_short[i] = cs;
-    cnt_all[i] = cs + cl;
-    atomicMax(&scal->max_neighbors, cs + cl);
-    atomicMax(&scal->max_short, cs);
-    atomicMax(&scal->max_long, cl);
-    if (cs > cap_s || cl > cap_l) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+        if (!active) continue;
+        if ((cs & 3) != 0 && cs < cap_s) ls[(size_t)(cs >> 2) * n] = make_uint4(s0, s1, s2, s3);
+        if ((cl & 3) != 0 && cl < cap_l) ll[(size_t)(cl >> 2) * n] = make_uint4(l0, l1, l2, l3);
+        if (is_wall && !any_fluid) cs = cl = 0;
+        cnt_short[i] = cs;
+        cnt_all[i] = cs + cl;
+        atomicMax(&scal->max_neighbors, cs + cl);
+        atomicMax(&scal->max_short, cs);
+        atomicMax(&scal->max_long, cl);
+        if (cs > cap_s || cl > cap_l) atomicOr(&scal->flags, DEVFLAG_NEIGHBOR_OVERFLOW);
+    }
 }
 
 // ---- per step -----------------------------------------------------------------
@@ -845,7 +869,8 @@ int mixed_rebuild(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, 
     for (int attempt = 0; attempt < 3; ++attempt) {
         MTRY(cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), s));
         MTRY(cudaMemsetAsync(&d.scal->max_short, 0, 2 * sizeof(int), s));
-        k_mix_list<<<blocks(n, 128), 128, 0, s>>>(c, m->mc, m->p32, d.keys, d.cellstart, m->list, m->cap_l,
+        k_mix_list<<<blocks(2LL * c.tot, kMixListWarps), 32 * kMixListWarps, 0, s>>>(c, m->mc, m->p32, d.cellstart,
+                                                                                   m->list, m->cap_l,
                                                   m->cnt_short, m->cnt_all, d.scal);
         ++nl;
         MTRY(cudaGetLastError());

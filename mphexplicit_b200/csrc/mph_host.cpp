@@ -466,7 +466,7 @@ static int rebuild_fp64(mph_ctx* ctx) {
         {
             Launch L(ctx, "neighbor_list");
             mph::launch_pos32(s, d.pos[d.cur], d.pos32, st);
-            mph::launch_neighbor_list(s, d.pos[d.cur], d.pos32, d.keys, d.cellstart, d.ncount, d.nlist, d.cap,
+            mph::launch_neighbor_list(s, d.pos[d.cur], d.pos32, d.cellstart, d.ncount, d.nlist, d.cap,
                                       sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.cap_s, d.scal, st);
             L.count = 2;
         }

@@ -120,11 +120,12 @@ Prefilter make_prefilter(const SimConst& c);
 // FP32 positions relative to the domain origin (the prefilter's input).
 void launch_pos32(const SimConst& c, const double4* pos, float4* pos32, cudaStream_t s);
 // nlist_s != nullptr: also the short sublist (entries within rs2, in list
-// order; its longest length in scal->max_short).  pos32 != nullptr: the FP32
-// prefilter skips candidates surely beyond the cut-off (same list).
-void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* keys,
-                          const int* cellstart, int* ncount, int* nlist, int cap,
-                          int* ncount_s, int* nlist_s, int cap_s, StepScalars* scal, cudaStream_t s);
+// order; its longest length in scal->max_short).  pos32 (launch_pos32) feeds
+// the FP32 prefilter that skips candidates surely beyond the cut-off (the
+// list is the same).  One warp per cell key.
+void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* pos32, const int* cellstart,
+                          int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
+                          StepScalars* scal, cudaStream_t s);
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);
 void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s);
 
