@@ -83,6 +83,7 @@ struct mph_ctx {
     bool virial_valid = false;
     bool dens_a_valid = false;  // DensityA / PressureA hold the values of the last step
     bool wall_force_valid = true;  // the walls' Force holds the values of the last step
+    int lazy_pos = -1;             // pos buffer holding the last step's positions after mph_set_state
     int max_neighbors = 0;
     long long launches = 0;
     Profiler prof;
@@ -494,15 +495,22 @@ static void sweep_a(mph_ctx* ctx, bool advance_wall) {
                         d.dens_a, d.strain_p, d.div_p, d.press, d.gc, advance_wall ? d.wall_center : nullptr,
                         ctx->stream);
     ctx->dens_a_valid = ctx->sc.has_st;  // without surface tension, computed when read
+    ctx->lazy_pos = -1;                  // this step's positions are the current ones
 }
 
 // DensityA / PressureA of the last step, for a reader (FP64 and learned forms
 // without surface tension, where the step itself does not need them).
+// The positions the last step used: the current ones, or their copy when
+// mph_set_state has replaced them since.
+static const double4* step_positions(mph_ctx* ctx) {
+    return ctx->d.pos[ctx->lazy_pos >= 0 ? ctx->lazy_pos : ctx->d.cur];
+}
+
 static void ensure_density_a(mph_ctx* ctx) {
     if (ctx->mixed || ctx->dens_a_valid) return;
     mph::DevFP64& d = ctx->d;
     Launch L(ctx, "density_a");
-    mph::launch_density_a(ctx->sc, d.pos[d.cur], d.ncount, d.nlist, d.dens_a, d.gc, ctx->stream);
+    mph::launch_density_a(ctx->sc, step_positions(ctx), d.ncount, d.nlist, d.dens_a, d.gc, ctx->stream);
     ctx->dens_a_valid = true;
 }
 
@@ -512,8 +520,8 @@ static void ensure_wall_force(mph_ctx* ctx) {
     if (ctx->mixed || ctx->wall_force_valid) return;
     mph::DevFP64& d = ctx->d;
     Launch L(ctx, "wall_force");
-    mph::launch_sweep_b(ctx->sc, d.cellstart, d.pos[d.cur], nullptr, nullptr, d.press, d.gc, d.ncount, d.nlist,
-                        d.force, d.scal, ctx->stream, nullptr, nullptr, nullptr, 2);
+    mph::launch_sweep_b(ctx->sc, d.cellstart, step_positions(ctx), nullptr, nullptr, d.press, d.gc, d.ncount,
+                        d.nlist, d.force, d.scal, ctx->stream, nullptr, nullptr, nullptr, 2);
     ctx->wall_force_valid = true;
 }
 
@@ -1019,11 +1027,17 @@ extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, doubl
 
 extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
-    ensure_density_a(ctx);  // from the positions the last step used, before they are replaced
-    ensure_wall_force(ctx);
     mph::DevFP64& d = ctx->d;
     const size_t n = (size_t)ctx->n;
     cudaStream_t st = ctx->stream;
+    // The last step's output-only fields (DensityA without surface tension, the
+    // walls' Force) are computed when read, from the positions that step used:
+    // keep a copy of those in the idle ping-pong buffer before they are replaced.
+    if (xyz && !ctx->mixed && ctx->lazy_pos < 0 && (!ctx->dens_a_valid || !ctx->wall_force_valid)) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(d.pos[1 - d.cur], d.pos[d.cur], n * sizeof(double4), cudaMemcpyDeviceToDevice,
+                                      st));
+        ctx->lazy_pos = 1 - d.cur;
+    }
     if (xyz) {
         CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
         Launch L(ctx, "unpack3");
