@@ -85,15 +85,26 @@ def measured_bf16_peak():
     return 1590.0, "fallback (MEASURED_PEAKS.json absent)"
 
 
-def ncu_traffic(kernel: str, mode: str):
-    """DRAM bytes per step of the `kernel` scope on the full-size dam break,
-    from the committed ncu summary (profiles/), or None."""
+def _profile_value(kernel: str, key: str):
     tag = kernel + ("_fp32" if kernel == "mix_sweep_b" else "")  # one FP32 force sweep in both mixed forms
     p = os.path.join(ROOT, "profiles", "ncu_%s_dam_break_3d.md" % tag)
     if not os.path.exists(p):
         return None
-    m = re.search(r"traffic_bytes_per_step_full_size:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(key + r":\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
+
+
+def ncu_traffic(kernel: str, mode: str):
+    """DRAM bytes per step of the `kernel` scope on the full-size dam break,
+    from the committed ncu summary (profiles/), or None."""
+    return _profile_value(kernel, "traffic_bytes_per_step_full_size")
+
+
+def ncu_pipe(kernel: str):
+    """The busiest execution pipe of `kernel` and its active fraction (ncu
+    sm__pipe_*_cycles_active of the committed summary), or None."""
+    f = _profile_value(kernel, "fp64_pipe_active_frac")
+    return {"pipe": "fp64", "active_frac": f, "source": "ncu sm__pipe_fp64_cycles_active, profiles/"} if f else None
 
 
 class ClockSampler:
@@ -600,7 +611,8 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
     algo = ALGO_BYTES.get(name, 0.0) * units
     achieved = algo / avg_s / 1e9
     out["roofline"] = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                       "frac": achieved / peak, "traffic": ncu_traffic(name, mode) if args.scene == "dam" else None, "peak_source": peak_kind,
+                       "frac": achieved / peak, "traffic": ncu_traffic(name, mode) if args.scene == "dam" else None,
+                       "compute_bound": ncu_pipe(name), "peak_source": peak_kind,
                        "algorithmic_bytes_per_step": algo, "particles_per_step": units,
                        "launches_per_step": nl / args.steps, "ms_per_step": avg_s * 1e3,
                        "kernels_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()}}
