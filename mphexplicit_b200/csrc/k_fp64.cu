@@ -288,11 +288,19 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
 // terms are not evaluated; fluid particle i adds instead the sum of its
 // edge-MLP pair forces eforce[eoff[i] .. eoff[i+1]) (FP32, in edge order),
 // which is also stored in lsum[i].
-template <bool ST, bool RATIO, bool LRN>
+// SPLIT (no surface tension, not learned): the PressureP force visits only
+// pairs within RadiusP, all of which are in the short sublist, in list order
+// (the argument of k_neighbor_list), so that sum runs as its own loop over the
+// short sublist and the main loop carries ViscosityV alone.  The terms and
+// their order in each sum are the reference's; the main loop no longer runs
+// the pressure block under a branch that some lane takes on nearly every
+// entry while most lanes wait.
+template <bool ST, bool RATIO, bool LRN, bool SPLIT>
 __global__ void __launch_bounds__(128, MPH_SWEEPB_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
           const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
-          const int* __restrict__ ncount, const int* __restrict__ nlist, double4* __restrict__ force,
+          const int* __restrict__ ncount, const int* __restrict__ nlist, const int* __restrict__ ncount_s,
+          const int* __restrict__ nlist_s, double4* __restrict__ force,
           StepScalars* __restrict__ scal, const int* __restrict__ eoff, const float4* __restrict__ eforce,
           float4* __restrict__ lsum, int part) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -317,6 +325,34 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     double fa0 = 0.0, fa1 = 0.0, fa2 = 0.0;
     double fd0 = 0.0, fd1 = 0.0, fd2 = 0.0;
     double fv0 = 0.0, fv1 = 0.0, fv2 = 0.0;
+    if (SPLIT) {  // PressureP force (main.cpp:1908-1938) over the short sublist
+        const int cs = ncount_s[i];
+        const int* lq = nlist_s + i;
+        int q1 = cs > 0 ? __ldg(lq) : i;
+        lq += n;
+        for (int k = 0; k < cs; ++k) {
+            const int j = q1;
+            if (k + 1 < cs) q1 = __ldg(lq);
+            lq += n;
+            if (j == i) continue;
+            const double4 pj = pos[j];
+            double x[3];
+            disp(c, pi, pj, x);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            if (!(r2 < c.rp2)) continue;
+            const double r = sqrt(r2);
+            const double ri = __drcp_rn(r);
+            const double pjp = velp[j].w;  // PressureP of j
+            const double qp = div_rs(r, c.rp, c.inv_rp);
+            const double dw = s_dwp(c, qp);
+            const double gw0 = div_rs(dw * x[0], r, ri), gw1 = div_rs(dw * x[1], r, ri),
+                         gw2 = div_rs(dw * x[2], r, ri);
+            const double ps = vi.w + pjp;
+            fp0 += ps * gw0 * c.vol;
+            fp1 += ps * gw1 * c.vol;
+            fp2 += ps * gw2 * c.vol;
+        }
+    }
     // software pipeline: list indices two entries ahead, the neighbour's two
     // records (position, velocity + PressureP) one entry ahead, so their
     // gathers overlap the previous pair's FP64 arithmetic
@@ -344,7 +380,7 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         // PressureA term adds a signed zero to a sum that starts at +0: the sum
         // stays +0 exactly, so the term is skipped (ST == false).
         // R*R - r2 > 0 (main.cpp:1926 and the other force sums) is r2 < R*R
-        const bool in_p = r2 < c.rp2;
+        const bool in_p = !SPLIT && r2 < c.rp2;
         const bool in_a = !LRN && ST && (r2 < c.ra2);
         const bool in_g = !LRN && ST && (r2 < c.rg2);
         const bool in_v = !LRN && r2 < c.rv2;
@@ -810,15 +846,17 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
                     double4* vel_out, const double4* press, const double4* gc, const int* ncount,
-                    const int* nlist, double4* force, StepScalars* scal, cudaStream_t s, const int* eoff,
-                    const float4* eforce, float4* lsum, int part) {
+                    const int* nlist, const int* ncount_s, const int* nlist_s, double4* force, StepScalars* scal,
+                    cudaStream_t s, const int* eoff, const float4* eforce, float4* lsum, int part) {
     (void)vel_in;
     const int nb = blocks(c.n, 128);
-#define SWEEP_B(ST, RATIO, LRN) \
-    k_sweep_b<ST, RATIO, LRN><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist, force, scal, \
-                                                 eoff, eforce, lsum, part)
-#define SWEEP_B2(ST, RATIO) \
-    if (eforce) SWEEP_B(ST, RATIO, true); else SWEEP_B(ST, RATIO, false)
+#define SWEEP_B(ST, RATIO, LRN, SPLIT) \
+    k_sweep_b<ST, RATIO, LRN, SPLIT><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist,        \
+                                                        ncount_s, nlist_s, force, scal, eoff, eforce, lsum, part)
+#define SWEEP_B2(ST, RATIO)                                             \
+    if (eforce) SWEEP_B(ST, RATIO, true, false);                        \
+    else if (!ST && nlist_s) SWEEP_B(ST, RATIO, false, !ST);            \
+    else SWEEP_B(ST, RATIO, false, false)
     if (c.has_st) {
         if (c.ratio_all_one) { SWEEP_B2(true, false); } else { SWEEP_B2(true, true); }
     } else {

@@ -520,8 +520,10 @@ static void ensure_wall_force(mph_ctx* ctx) {
     if (ctx->mixed || ctx->wall_force_valid) return;
     mph::DevFP64& d = ctx->d;
     Launch L(ctx, "wall_force");
+    const bool sl = uses_short_list(ctx);
     mph::launch_sweep_b(ctx->sc, d.cellstart, step_positions(ctx), nullptr, nullptr, d.press, d.gc, d.ncount,
-                        d.nlist, d.force, d.scal, ctx->stream, nullptr, nullptr, nullptr, 2);
+                        d.nlist, sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force, d.scal, ctx->stream,
+                        nullptr, nullptr, nullptr, 2);
     ctx->wall_force_valid = true;
 }
 
@@ -669,8 +671,10 @@ static int step_fp64(mph_ctx* ctx, int nsteps) {
         sweep_a(ctx, true);
         {
             Launch L(ctx, "sweep_b");
+            const bool sl = uses_short_list(ctx);
             mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.vel[1 - d.vcur], d.press, d.gc,
-                                d.ncount, d.nlist, d.force, d.scal, st, nullptr, nullptr, nullptr, 1);
+                                d.ncount, d.nlist, sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force,
+                                d.scal, st, nullptr, nullptr, nullptr, 1);
             ctx->wall_force_valid = false;  // computed when read
         }
         d.vcur = 1 - d.vcur;
@@ -778,8 +782,9 @@ static int learned_buffers(mph_ctx* ctx) {
 static void plain_sweep_b(mph_ctx* ctx, double4* vel_out, double4* force) {
     mph::DevFP64& d = ctx->d;
     Launch L(ctx, "sweep_b");
+    const bool sl = uses_short_list(ctx);
     mph::launch_sweep_b(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vel_out, d.press, d.gc, d.ncount, d.nlist,
-                        force, d.scal, ctx->stream);
+                        sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, force, d.scal, ctx->stream);
 }
 
 // The FP64 step with the learned pair terms, the judge and the fallback.
@@ -835,8 +840,8 @@ static int step_learned(mph_ctx* ctx, int nsteps) {
                 // the learned sweep evaluates only the pairs within RadiusP
                 const bool sl = uses_short_list(ctx);
                 mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vout, d.press, d.gc,
-                                    sl ? d.ncount_s : d.ncount, sl ? d.nlist_s : d.nlist, d.force, d.scal, st,
-                                    L.eoff, L.eforce, L.lsum);
+                                    sl ? d.ncount_s : d.ncount, sl ? d.nlist_s : d.nlist, nullptr, nullptr,
+                                    d.force, d.scal, st, L.eoff, L.eforce, L.lsum);
             }
             bool use = true;
             if (L.info.steps % L.judge_interval == 0) {

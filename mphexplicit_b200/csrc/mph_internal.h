@@ -148,11 +148,14 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 // needs only the pairs within RadiusP, so the short sublist may be passed).
 // part: 0 every particle; 1 the fluid (walls copy their velocity, their
 // force is not written); 2 the walls' forces alone (vel_out unused).
+// ncount_s / nlist_s (no surface tension, not learned): the short sublist,
+// over which the PressureP force runs as its own loop (same result).
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel_in, double4* vel_out, const double4* press,
-                    const double4* gc, const int* ncount, const int* nlist, double4* force,
-                    StepScalars* scal, cudaStream_t s, const int* eoff = nullptr,
-                    const float4* eforce = nullptr, float4* lsum = nullptr, int part = 0);
+                    const double4* gc, const int* ncount, const int* nlist, const int* ncount_s,
+                    const int* nlist_s, double4* force, StepScalars* scal, cudaStream_t s,
+                    const int* eoff = nullptr, const float4* eforce = nullptr, float4* lsum = nullptr,
+                    int part = 0);
 
 // ---- learned form (k_fp64.cu) ---------------------------------------------
 // CSR edges of the fluid particles' lists (i < nf): eoff[0..nf] = exclusive
