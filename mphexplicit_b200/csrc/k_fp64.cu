@@ -18,11 +18,12 @@
 
 // Resident 128-thread blocks per SM the sweeps are compiled for (register cap
 // 65536 / (128 * blocks)); latency hiding vs. spills, set by measurement on
-// the full dam break: sweep A 8 (64 registers); the force sweep, which keeps
-// the next neighbour's records in flight, 5 (94 registers, no spills: 3.46 ms
-// against 3.69 ms without the prefetch at 7 blocks, 4.21 ms with it at 6).
+// the full dam break.  Both sweeps keep the next neighbour's records in
+// flight: sweep A at 7 (72 registers; at 8 it spills), the force sweep at 5
+// (90 registers, no spills: 3.46 ms against 3.69 ms without the prefetch at 7
+// blocks, 4.21 ms with it at 6, before its pressure loop was split off).
 #ifndef MPH_SWEEP_MINB
-#define MPH_SWEEP_MINB 8
+#define MPH_SWEEP_MINB 7
 #endif
 #ifndef MPH_SWEEPB_MINB
 #define MPH_SWEEPB_MINB 5
@@ -183,14 +184,24 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
     const size_t n = (size_t)c.n;
     double sum_a = 0.0, sum_p = 0.0, sum_d = 0.0;
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    // indices two entries ahead, the neighbour's position and velocity one ahead
     const int* lp = nlist + i;
-    int jn = cnt > 0 ? __ldg(lp) : 0;  // next index, loaded one iteration ahead
+    int j1 = cnt > 0 ? __ldg(lp) : i;
+    int j2 = cnt > 1 ? __ldg(lp + n) : i;
+    lp += 2 * n;
+    double4 pn = pos[j1], vq = vel[j1];
     for (int k = 0; k < cnt; ++k) {
-        const int j = jn;
+        const int j = j1;
+        const double4 pj = pn;
+        const double4 vjn = vq;
+        j1 = j2;
+        if (k + 2 < cnt) j2 = __ldg(lp);
         lp += n;
-        if (k + 1 < cnt) jn = __ldg(lp);
+        if (k + 1 < cnt) {
+            pn = pos[j1];
+            vq = vel[j1];
+        }
         if (j == i) continue;
-        const double4 pj = pos[j];
         double x[3];
         disp(c, pi, pj, x);
         const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
@@ -221,8 +232,7 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
             const double dw = s_dwp(c, qp);
             const double ri = __drcp_rn(r);
             const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
-            const double4 vj = vel[j];
-            const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+            const double u0 = vjn.x - vi.x, u1 = vjn.y - vi.y, u2 = vjn.z - vi.z;
             sum_d -= u0 * e0 * dw;
             sum_d -= u1 * e1 * dw;
             sum_d -= u2 * e2 * dw;
@@ -326,23 +336,32 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     double fd0 = 0.0, fd1 = 0.0, fd2 = 0.0;
     double fv0 = 0.0, fv1 = 0.0, fv2 = 0.0;
     if (SPLIT) {  // PressureP force (main.cpp:1908-1938) over the short sublist
+        // indices two entries ahead, the neighbour's records one entry ahead
         const int cs = ncount_s[i];
         const int* lq = nlist_s + i;
         int q1 = cs > 0 ? __ldg(lq) : i;
-        lq += n;
+        int q2 = cs > 1 ? __ldg(lq + n) : i;
+        lq += 2 * n;
+        double4 qn = pos[q1];
+        double qp1 = velp[q1].w;
         for (int k = 0; k < cs; ++k) {
             const int j = q1;
-            if (k + 1 < cs) q1 = __ldg(lq);
+            const double4 pj = qn;
+            const double pjp = qp1;  // PressureP of j
+            q1 = q2;
+            if (k + 2 < cs) q2 = __ldg(lq);
             lq += n;
+            if (k + 1 < cs) {
+                qn = pos[q1];
+                qp1 = velp[q1].w;
+            }
             if (j == i) continue;
-            const double4 pj = pos[j];
             double x[3];
             disp(c, pi, pj, x);
             const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
             if (!(r2 < c.rp2)) continue;
             const double r = sqrt(r2);
             const double ri = __drcp_rn(r);
-            const double pjp = velp[j].w;  // PressureP of j
             const double qp = div_rs(r, c.rp, c.inv_rp);
             const double dw = s_dwp(c, qp);
             const double gw0 = div_rs(dw * x[0], r, ri), gw1 = div_rs(dw * x[1], r, ri),
