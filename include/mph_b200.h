@@ -247,6 +247,19 @@ int mph_get_state(mph_ctx* ctx, int* particle_index, int* type,
  * Used by callers that keep the state on the host between steps. */
 int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel);
 
+/* mph_step(ctx, nsteps), then the positions and velocities after the last
+ * step into xyz[n][3] and vel[n][3] (sorted order; either may be NULL): the
+ * same values as mph_step + mph_get_state, for callers that read the state
+ * every step (main.cpp:404-431 writes it at output times).  In the FP64 form
+ * the copies overlap the last step: the positions are final once its move
+ * and any list rebuild are done and are copied while the sweeps run; when
+ * vel is pinned and mapped (cudaHostAlloc memory, or cudaHostRegister with
+ * cudaHostRegisterMapped) the force sweep stores each new velocity into it
+ * directly as it computes it.  Pageable buffers give the same values with
+ * less overlap.  The other forms step, then copy.  Returns after the copies
+ * have landed. */
+int mph_step_read_state(mph_ctx* ctx, int nsteps, double* xyz, double* vel);
+
 /* Secondary per-particle fields in sorted order (any pointer may be NULL):
  * DivergenceP, PressureP, PressureA, GravityCenter[3]. */
 int mph_get_fields(mph_ctx* ctx, double* divergence_p, double* pressure_p,

@@ -305,6 +305,37 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
 // their order in each sum are the reference's; the main loop no longer runs
 // the pressure block under a branch that some lane takes on nearly every
 // entry while most lanes wait.
+// Row i of an [n][3] FP64 array in pinned host memory mapped into the device
+// (the velocity read-back of mph_step_read_state).  When the 32 lanes of the
+// warp are here together with consecutive rows (an even first row, so the
+// warp's 768 bytes start on a 16-byte boundary of a 16-byte aligned array),
+// the rows go through the warp's 96-double stage in shared memory and out as
+// 16-byte stores covering whole 128-byte lines: full-line writes over PCIe
+// instead of 8-byte pieces.  Otherwise each lane stores its own three values.
+__device__ __forceinline__ void store_host_row3(double* __restrict__ out, int i, double x, double y, double z,
+                                                double* __restrict__ stage) {
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31;
+    if (m == 0xffffffffu) {
+        const int first = __shfl_sync(m, i, 0);
+        if (__all_sync(m, i == first + lane) && (first & 1) == 0) {
+            stage[3 * lane] = x;
+            stage[3 * lane + 1] = y;
+            stage[3 * lane + 2] = z;
+            __syncwarp(m);
+            double2* dst = reinterpret_cast<double2*>(out + 3 * (size_t)first);
+            const double2* src = reinterpret_cast<const double2*>(stage);
+            dst[lane] = src[lane];
+            if (lane < 16) dst[32 + lane] = src[32 + lane];
+            __syncwarp(m);
+            return;
+        }
+    }
+    out[3 * (size_t)i] = x;
+    out[3 * (size_t)i + 1] = y;
+    out[3 * (size_t)i + 2] = z;
+}
+
 template <bool ST, bool RATIO, bool LRN, bool SPLIT>
 __global__ void __launch_bounds__(128, MPH_SWEEPB_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
@@ -312,15 +343,18 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
           const int* __restrict__ ncount, const int* __restrict__ nlist, const int* __restrict__ ncount_s,
           const int* __restrict__ nlist_s, double4* __restrict__ force,
           StepScalars* __restrict__ scal, const int* __restrict__ eoff, const float4* __restrict__ eforce,
-          float4* __restrict__ lsum, int part) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+          float4* __restrict__ lsum, int part, int i0, int i1, double* __restrict__ vel_host) {
+    __shared__ __align__(16) double vstage[4][96];  // store_host_row3, one stage per warp
+    double* const stage = vstage[threadIdx.x >> 5];
+    const int i = i0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);  // particles [i0, i1)
+    if (i >= i1) return;
     const int nf = cellstart[c.tot];
     const double4 vi = velp[i];   // .w = PressureP
     // part 1: fluid only; a wall keeps its velocity (what the full sweep
     // writes for it) and its force is left for part 2 (output only)
     if (part == 1 && i >= nf) {
         vel_out[i] = make_double4(vi.x, vi.y, vi.z, 0.0);
+        if (vel_host) store_host_row3(vel_host, i, vi.x, vi.y, vi.z, stage);
         return;
     }
     if (part == 2 && i < nf) return;
@@ -494,7 +528,11 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
         if (!(isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
     }
     force[i] = make_double4(F0, F1, F2, 0.0);
-    if (part != 2) vel_out[i] = vn;
+    if (part != 2) {
+        vel_out[i] = vn;
+        // mapped pinned host memory: the read-back travels while the sweep runs
+        if (vel_host) store_host_row3(vel_host, i, vn.x, vn.y, vn.z, stage);
+    }
 }
 
 // Self-check of div_rn against the hardware IEEE division: operands with
@@ -866,12 +904,16 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel_in,
                     double4* vel_out, const double4* press, const double4* gc, const int* ncount,
                     const int* nlist, const int* ncount_s, const int* nlist_s, double4* force, StepScalars* scal,
-                    cudaStream_t s, const int* eoff, const float4* eforce, float4* lsum, int part) {
+                    cudaStream_t s, const int* eoff, const float4* eforce, float4* lsum, int part, int i0,
+                    int i1, double* vel_host) {
     (void)vel_in;
-    const int nb = blocks(c.n, 128);
+    if (i1 < 0) i1 = c.n;
+    if (i1 <= i0) return;
+    const int nb = blocks(i1 - i0, 128);
 #define SWEEP_B(ST, RATIO, LRN, SPLIT) \
     k_sweep_b<ST, RATIO, LRN, SPLIT><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist,        \
-                                                        ncount_s, nlist_s, force, scal, eoff, eforce, lsum, part)
+                                                        ncount_s, nlist_s, force, scal, eoff, eforce, lsum, part, \
+                                                        i0, i1, vel_host)
 #define SWEEP_B2(ST, RATIO)                                             \
     if (eforce) SWEEP_B(ST, RATIO, true, false);                        \
     else if (!ST && nlist_s) SWEEP_B(ST, RATIO, false, !ST);            \

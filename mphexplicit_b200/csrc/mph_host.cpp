@@ -64,6 +64,14 @@ struct LearnedState {
     mph_learned_info info{};
 };
 
+// mph_step_read_state: the copy stream (packs and device-to-host copies), its
+// events and the velocities' staging buffer; made by the first call.
+struct ReadBack {
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ev[2] = {};
+    double* stage_v = nullptr;  // [n][3]
+};
+
 struct mph_ctx {
     int mode = MPH_MODE_FP64;
     int n_fluid = 0;
@@ -86,6 +94,7 @@ struct mph_ctx {
     int lazy_pos = -1;             // pos buffer holding the last step's positions after mph_set_state
     int max_neighbors = 0;
     long long launches = 0;
+    ReadBack rb;
     Profiler prof;
     std::string err;
     mph::TextWriter* text = nullptr;  // *.prof / *.vtk writer thread, made by the first write
@@ -559,6 +568,14 @@ extern "C" void mph_destroy(mph_ctx* ctx) {
         if (L.h_sums) cudaFreeHost(L.h_sums);
     }
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    {
+        ReadBack& R = ctx->rb;
+        if (R.copy) cudaStreamSynchronize(R.copy);
+        for (cudaEvent_t e : R.ev)
+            if (e) cudaEventDestroy(e);
+        cudaFree(R.stage_v);
+        if (R.copy) cudaStreamDestroy(R.copy);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -650,24 +667,35 @@ static int check_flags(mph_ctx* ctx) {
     return MPH_OK;
 }
 
+// One FP64 step up to the pair sweeps: convection, wall motion, periodic wrap
+// and the displacement test, then the list rebuild when it fires
+// (main.cpp:387-403).  The positions are the step's final ones after this.
+static int step_fp64_head(mph_ctx* ctx) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+    {
+        Launch L(ctx, "move");
+        mph::launch_move(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap, d.wall_center, d.scal, st);
+    }
+    TRY(read_scalars(ctx));
+    TRY(check_flags(ctx));
+    double ms;
+    std::memcpy(&ms, &ctx->h_scal->max_shift2_bits, sizeof(double));
+    if (ms > s.shift_thr) {  // neighborCalculation() == 1 (main.cpp:1102)
+        TRY(rebuild_fp64(ctx));
+        ++ctx->rebuilds;
+    }
+    return MPH_OK;
+}
+
 static int step_fp64(mph_ctx* ctx, int nsteps) {
     mph::DevFP64& d = ctx->d;
     const SimConst& s = ctx->sc;
     cudaStream_t st = ctx->stream;
     for (int k = 0; k < nsteps; ++k) {
-        CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
-        {
-            Launch L(ctx, "move");
-            mph::launch_move(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap, d.wall_center, d.scal, st);
-        }
-        TRY(read_scalars(ctx));
-        TRY(check_flags(ctx));
-        double ms;
-        std::memcpy(&ms, &ctx->h_scal->max_shift2_bits, sizeof(double));
-        if (ms > s.shift_thr) {  // neighborCalculation() == 1 (main.cpp:1102)
-            TRY(rebuild_fp64(ctx));
-            ++ctx->rebuilds;
-        }
+        TRY(step_fp64_head(ctx));
         sweep_a(ctx, true);
         {
             Launch L(ctx, "sweep_b");
@@ -1030,6 +1058,93 @@ extern "C" int mph_get_state(mph_ctx* ctx, int* particle_index, int* type, doubl
     return MPH_OK;
 }
 
+static int readback_init(mph_ctx* ctx) {
+    ReadBack& R = ctx->rb;
+    if (R.copy) return MPH_OK;
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&R.copy, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : R.ev) CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TRY(dalloc(ctx, &R.stage_v, 3 * (size_t)ctx->n));
+    return MPH_OK;
+}
+
+// The device address of a host buffer of `count` doubles when all of it is
+// pinned and mapped (cudaHostAlloc memory always is under unified addressing;
+// cudaHostRegister memory when registered mapped), else nullptr.
+static double* mapped_host(double* p, size_t count) {
+    if (!p || count == 0) return nullptr;
+    cudaPointerAttributes a{}, b{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || cudaPointerGetAttributes(&b, p + count - 1) != cudaSuccess) {
+        cudaGetLastError();  // pageable memory on older runtimes reports an error: not an error here
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+        return nullptr;
+    if ((char*)b.devicePointer - (char*)a.devicePointer != (ptrdiff_t)((count - 1) * sizeof(double))) return nullptr;
+    if (((uintptr_t)a.devicePointer & 15u) != 0) return nullptr;  // the sweep's 16-byte stores
+    return (double*)a.devicePointer;
+}
+
+// The FP64 form's last step with its read-back overlapped.  The positions are
+// final once the move and any rebuild are done: they are packed and copied on
+// a copy stream while the sweeps run.  The velocities: with a pinned, mapped
+// host buffer the force sweep stores each particle's new velocity into it as
+// well as into device memory (24 B per particle over PCIe while the sweep
+// runs); otherwise they are packed and copied after the sweep.  Same kernels
+// and inputs: the bits of mph_step + mph_get_state.
+static int step_fp64_read(mph_ctx* ctx, double* xyz, double* vel) {
+    TRY(readback_init(ctx));
+    ReadBack& R = ctx->rb;
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    const size_t n = (size_t)ctx->n;
+    double* vh = mapped_host(vel, 3 * n);
+    TRY(step_fp64_head(ctx));
+    CUDA_TRY(ctx, cudaEventRecord(R.ev[0], st));  // positions final
+    sweep_a(ctx, true);
+    double4* vout = d.vel[1 - d.vcur];
+    {
+        Launch L(ctx, "sweep_b");
+        const bool sl = uses_short_list(ctx);
+        mph::launch_sweep_b(s, d.cellstart, d.pos[d.cur], d.vel[d.vcur], vout, d.press, d.gc, d.ncount, d.nlist,
+                            sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force, d.scal, st, nullptr,
+                            nullptr, nullptr, 1, 0, -1, vh);
+        ctx->wall_force_valid = false;  // computed when read
+    }
+    CUDA_TRY(ctx, cudaEventRecord(R.ev[1], st));  // velocities final
+    // copies, enqueued after the compute so pageable buffers do not hold it back
+    if (xyz) {
+        CUDA_TRY(ctx, cudaStreamWaitEvent(R.copy, R.ev[0], 0));
+        mph::launch_pack3(ctx->n, d.pos[d.cur], d.staging, R.copy);
+        ++ctx->launches;
+        CUDA_TRY(ctx, cudaMemcpyAsync(xyz, d.staging, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, R.copy));
+    }
+    if (vel && !vh) {
+        CUDA_TRY(ctx, cudaStreamWaitEvent(R.copy, R.ev[1], 0));
+        mph::launch_pack3(ctx->n, vout, R.stage_v, R.copy);
+        ++ctx->launches;
+        CUDA_TRY(ctx, cudaMemcpyAsync(vel, R.stage_v, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, R.copy));
+    }
+    d.vcur = 1 - d.vcur;
+    CUDA_TRY(ctx, cudaGetLastError());
+    ctx->time += ctx->p.dt;  // main.cpp:449
+    ++ctx->step;
+    ctx->virial_valid = false;
+    CUDA_TRY(ctx, cudaStreamSynchronize(R.copy));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return MPH_OK;
+}
+
+extern "C" int mph_step_read_state(mph_ctx* ctx, int nsteps, double* xyz, double* vel) {
+    if (!ctx || nsteps < 1) return fail(ctx, MPH_ERR_ARG, "bad arguments");
+    if (ctx->mixed || ctx->mode == MPH_MODE_LEARNED) {  // no overlap: the step, then the read
+        TRY(mph_step(ctx, nsteps));
+        return mph_get_state(ctx, nullptr, nullptr, xyz, vel, nullptr, nullptr, nullptr, nullptr, nullptr);
+    }
+    if (nsteps > 1) TRY(step_fp64(ctx, nsteps - 1));
+    return step_fp64_read(ctx, xyz, vel);
+}
+
 extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
     mph::DevFP64& d = ctx->d;
@@ -1043,15 +1158,22 @@ extern "C" int mph_set_state(mph_ctx* ctx, const double* xyz, const double* vel)
                                       st));
         ctx->lazy_pos = 1 - d.cur;
     }
+    // with the read-back's velocity buffer (made by mph_step_read_state) both
+    // copies are queued before the unpacks, back to back on the copy engine
+    double* sv = (xyz && vel && ctx->rb.stage_v) ? ctx->rb.stage_v : nullptr;
+    if (xyz) CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (sv) CUDA_TRY(ctx, cudaMemcpyAsync(sv, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
     if (xyz) {
-        CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, xyz, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
         Launch L(ctx, "unpack3");
         mph::launch_unpack3(ctx->n, d.staging, d.pos[d.cur], d.type[d.cur], st);
     }
     if (vel) {
-        CUDA_TRY(ctx, cudaMemcpyAsync(d.staging, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (!sv) {
+            sv = d.staging;
+            CUDA_TRY(ctx, cudaMemcpyAsync(sv, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
         Launch L(ctx, "unpack3");
-        mph::launch_unpack3(ctx->n, d.staging, d.vel[d.vcur], nullptr, st);
+        mph::launch_unpack3(ctx->n, sv, d.vel[d.vcur], nullptr, st);
     }
     if (ctx->mixed) TRY(mph::mixed_import(ctx->mixed, ctx->sc, ctx->d, st, &ctx->err));
     CUDA_TRY(ctx, cudaGetLastError());

@@ -150,12 +150,17 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 // force is not written); 2 the walls' forces alone (vel_out unused).
 // ncount_s / nlist_s (no surface tension, not learned): the short sublist,
 // over which the PressureP force runs as its own loop (same result).
+// [i0, i1): the particles (sorted order) this launch computes; i1 < 0 means
+// all n.  Every particle's result depends on the inputs alone, so a sweep
+// split into ranges gives the same bits as one launch.  vel_host (part 1): a
+// device-accessible [n][3] view of pinned host memory that also receives
+// each particle's new velocity.
 void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel_in, double4* vel_out, const double4* press,
                     const double4* gc, const int* ncount, const int* nlist, const int* ncount_s,
                     const int* nlist_s, double4* force, StepScalars* scal, cudaStream_t s,
                     const int* eoff = nullptr, const float4* eforce = nullptr, float4* lsum = nullptr,
-                    int part = 0);
+                    int part = 0, int i0 = 0, int i1 = -1, double* vel_host = nullptr);
 
 // ---- learned form (k_fp64.cu) ---------------------------------------------
 // CSR edges of the fluid particles' lists (i < nf): eoff[0..nf] = exclusive

@@ -310,6 +310,16 @@ class Solver:
         _check(self._lib.mph_get_state(self._ctx, None, None, _dp(xyz), _dp(vel), None, None, None, None, None),
                self._ctx)
 
+    def step_read_state(self, nsteps: int, xyz: np.ndarray | None, vel: np.ndarray | None) -> None:
+        """step(nsteps), then the positions and velocities after it into caller
+        arrays (sorted order, C-contiguous float64 [n, 3]); the FP64 form copies
+        them while its last step still computes (pinned arrays overlap fully)."""
+        for a in (xyz, vel):
+            if a is not None and not (a.dtype == np.float64 and a.flags.c_contiguous and a.size == 3 * self.n):
+                raise ValueError("xyz / vel must be C-contiguous float64 arrays of n x 3")
+        _check(self._lib.mph_step_read_state(self._ctx, int(nsteps), _dp(xyz) if xyz is not None else None,
+                                             _dp(vel) if vel is not None else None), self._ctx)
+
     def set_state(self, xyz: np.ndarray, vel: np.ndarray) -> None:
         _check(self._lib.mph_set_state(self._ctx, _dp(np.ascontiguousarray(xyz, np.float64)),
                                        _dp(np.ascontiguousarray(vel, np.float64))), self._ctx)

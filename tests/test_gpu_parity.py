@@ -179,6 +179,56 @@ def test_state_round_trip_and_step_continuity():
         assert_same(a.state()[key], b.state()[key], key)
 
 
+def _host_xv(n, pinned):
+    if not pinned:
+        return np.zeros((n, 3)), np.zeros((n, 3))
+    import torch
+    return (torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy(),
+            torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy())
+
+
+@pytest.mark.parametrize("name,pinned", [("dam_break_small", True), ("two_fluid_small", True),
+                                         ("moving_walls", False), ("droplet_2d", True)])
+def test_step_read_state_is_step_then_get_state(name, pinned):
+    """The overlapped step-and-read (force sweep in ranges on two streams, the
+    copies behind it) returns the bits of step + get_state, and a host loop of
+    step_read_state + set_state stays on the reference's trajectory."""
+    case = GoldenCase(name)
+    a, b = solver_for(case), solver_for(case)
+    x, v = _host_xv(a.n, pinned)
+    xb, vb = np.zeros((b.n, 3)), np.zeros((b.n, 3))
+    done, m = 0, 1
+    while done < case.steps:
+        m = min(m, case.steps - done)
+        a.step_read_state(m, x, v)
+        b.step(m)
+        b.get_xv(xb, vb)
+        assert_same(x, xb, "xyz")
+        assert_same(v, vb, "vel")
+        a.set_state(x, v)
+        done += m
+        m = m * 2 + 1
+    a.synchronize()
+    a.compute_virial()
+    st = a.state()
+    for key in STATE_KEYS:
+        assert_same(st[key], case.ref[key], key)
+
+
+def test_step_read_state_mixed_form():
+    """The mixed form has no overlapped path: it steps, then copies."""
+    case = GoldenCase("dam_break_small")
+    a, b = solver_for(case, "mixed"), solver_for(case, "mixed")
+    x, v = _host_xv(a.n, True)
+    xb, vb = np.zeros((b.n, 3)), np.zeros((b.n, 3))
+    for m in (1, 4):
+        a.step_read_state(m, x, v)
+        b.step(m)
+        b.get_xv(xb, vb)
+        assert_same(x, xb, "xyz")
+        assert_same(v, vb, "vel")
+
+
 def test_checkpoint_restart_is_the_reference_restart_exactly():
     """A checkpoint keeps the state in the order of the *.prof file of that
     time with the wall centres reached; restarting from it equals the
