@@ -668,13 +668,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "mixed_p64"],
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "mixed", "mixed_p64", "mixed_walk"],
                     help="headline form (default fp64: the reference's arithmetic, bit-exact); "
                          "all three are measured unless --only")
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=sorted(SCENES))
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,learned,batch,two_fluid,output",
+    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,mixed_walk,learned,batch,two_fluid,output",
                     help="forms to measure (comma list); the headline --mode must be among them for a full line")
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
@@ -717,7 +717,7 @@ def main():
         gpu_index = int(cvd)
     sc = make_scene(args, rank)
     wanted = [args.mode] if args.only else [f.strip() for f in args.forms.split(",") if f.strip()]
-    modes = [m for m in ("fp64", "mixed", "mixed_p64") if m in wanted]
+    modes = [m for m in ("fp64", "mixed", "mixed_p64", "mixed_walk") if m in wanted]
     res = {m: measure_form(args, sc, m, world, gpu_index, with_e2e=(m == args.mode)) for m in modes}
     forms = {}
     for m, r in res.items():

@@ -61,6 +61,14 @@ extern "C" {
  * 2.78 M-particle dam break, the same as MPH_MODE_MIXED's, whose density
  * sweep is faster). */
 #define MPH_MODE_MIXED_P64 2
+/* Flag for MPH_MODE_MIXED / MPH_MODE_MIXED_P64 (mode | MPH_MIXED_CELL_WALK):
+ * the force sweep reads no neighbour table: one warp per cell walks the 3^D
+ * stencil, keeps the candidates within the largest force radius of the box
+ * around its own particles, stages them in shared memory and evaluates each
+ * against every particle of the warp.  Same pair terms as the table sweep
+ * (within the same accuracy bound); the density sweep still reads the short
+ * part of the table. */
+#define MPH_MIXED_CELL_WALK 0x100
 /* The FP64 form with the viscosity and surface-tension pair terms
  * (ViscosityV main.cpp:1941-1985, DiffuseInterface :1778-1829, PressureA
  * force :1742-1775) replaced by an edge-MLP surrogate (mph_model) evaluated on

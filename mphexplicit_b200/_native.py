@@ -26,6 +26,7 @@ MODE_FP64 = 0
 MODE_MIXED = 1
 MODE_MIXED_P64 = 2
 MODE_LEARNED = 3
+MIXED_CELL_WALK = 0x100
 SAMPLE_FLOATS = 12
 
 _D4 = C.c_double * TYPE_COUNT

@@ -34,6 +34,10 @@ constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 #ifndef MPH_MIXB_MINB_FUSED
 #define MPH_MIXB_MINB_FUSED 8
 #endif
+// Resident 128-thread blocks per SM of the table-free force sweep.
+#ifndef MPH_WALK_MINB
+#define MPH_WALK_MINB 6
+#endif
 
 struct MixConst {
     int n, tot, dim, has_st, ratio_all_one, uniform_mu;
@@ -43,6 +47,7 @@ struct MixConst {
     float dhi[27][4];                  // cell-origin offset per code: hi part (on the grid)
     float dlo[27][4];                  //                              lo part
     float list_r2, short_r2;           // (MaxRadius+m)^2, (RP+m)^2
+    float walk_r2, walk_short2;        // cell walk: (largest force radius + s)^2, (RP + s)^2, s = 8 grid steps
     float ra2, rp2, rv2, rg2;
     float inv_ra, inv_rp, inv_rv, inv_rg;
     float ca, cp, cg, cv;              // (1/Sw)/h^D
@@ -675,6 +680,195 @@ k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4*
     vel_out[i] = v;
 }
 
+// The force sweep without the long table (MPH_MIXED_CELL_WALK).  One warp per
+// home key walks the 3^D stencil in the table build's order (main.cpp:
+// 1356-1392), reading each candidate range 32 records at a time (coalesced).
+// A lane keeps its candidate when the candidate's hi position lies within
+// the largest force radius of the bounding box of the warp's own particles;
+// the kept records go to the warp's stage in shared memory (compacted by a
+// ballot), and every lane evaluates every kept candidate against its own
+// particle, reading the stage with broadcast loads.  Pair terms as in k_mix_b:
+// where the hi-only distance is within RP (plus the hi/lo slack) the exact
+// hi/lo displacement and Kahan sums, beyond it the hi displacement and plain
+// sums.  Then gravity and the FP64 velocity update (main.cpp:1908-2010).  Wall
+// keys carry their velocities over (walls never accelerate).
+constexpr int kWalkWarps = 4;
+
+struct WalkRec {
+    float4 p;  // hi position + the cell offset's hi part (home-relative), type bits
+    float4 v;  // velocity, PressureP
+    float4 l;  // lo position + the cell offset's lo part, index bits
+};
+
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(32 * kWalkWarps, MPH_WALK_MINB)
+k_mix_b_walk(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ phl,
+             const float4* __restrict__ pv, const float4* __restrict__ gca, const double4* __restrict__ vel,
+             double4* __restrict__ vel_out, double4* __restrict__ force, StepScalars* __restrict__ scal) {
+    __shared__ WalkRec stage_all[kWalkWarps][32];
+    __shared__ float4 gstage_all[kWalkWarps][ST ? 32 : 1];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int key = blockIdx.x * kWalkWarps + wib;
+    if (key >= 2 * c.tot) return;  // whole warp
+    const int hb = cellstart[key], he = cellstart[key + 1];
+    if (hb == he) return;
+    if (key >= c.tot) {  // wall key
+        for (int i = hb + lane; i < he; i += 32) vel_out[i] = vel[i];
+        return;
+    }
+    WalkRec* const stage = stage_all[wib];
+    float4* const gstage = gstage_all[wib];
+    const int ic[3] = {key / (c.cc[1] * c.cc[2]), (key / c.cc[2]) % c.cc[1], key % c.cc[2]};
+    int jmin[3], w[3];
+    for (int d = 0; d < 3; ++d) {
+        const int r = c.range[d];
+        w[d] = 2 * r + 1;
+        const int b = (2 * r) - (ic[d] + r) % c.cc[d];
+        jmin[d] = b > 0 ? b : 0;
+    }
+    const float kInf = __int_as_float(0x7f800000);
+    for (int h0 = hb; h0 < he; h0 += 32) {
+        const int i = h0 + lane;
+        const bool act = i < he;
+        const int ii = act ? i : hb;
+        const float4 pi = phl[2 * (size_t)ii];
+        const float4 li = phl[2 * (size_t)ii + 1];
+        const float4 vi = pv[2 * (size_t)ii + 1];
+        const int ti = __float_as_int(pi.w);
+        float4 gi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ST) gi = gca[ii];
+        const float ai = m.a_k[ti];
+        const float mu_u = m.visc_mu[ti][ti];
+        // bounding box of the chunk's hi positions
+        float b0x = act ? pi.x : kInf, b0y = act ? pi.y : kInf, b0z = act ? pi.z : kInf;
+        float b1x = act ? pi.x : -kInf, b1y = act ? pi.y : -kInf, b1z = act ? pi.z : -kInf;
+        for (int o = 16; o > 0; o >>= 1) {
+            b0x = fminf(b0x, __shfl_xor_sync(0xffffffffu, b0x, o));
+            b0y = fminf(b0y, __shfl_xor_sync(0xffffffffu, b0y, o));
+            b0z = fminf(b0z, __shfl_xor_sync(0xffffffffu, b0z, o));
+            b1x = fmaxf(b1x, __shfl_xor_sync(0xffffffffu, b1x, o));
+            b1y = fmaxf(b1y, __shfl_xor_sync(0xffffffffu, b1y, o));
+            b1z = fmaxf(b1z, __shfl_xor_sync(0xffffffffu, b1z, o));
+        }
+        float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // within RP: Kahan
+        float gx = 0.f, gy = 0.f, gz = 0.f;                                 // beyond
+        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
+            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
+                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
+                    const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
+                    const int ncx = ((ic[0] - c.range[0] + ax) % c.cc[0] + c.cc[0]) % c.cc[0];
+                    const int ncy = ((ic[1] - c.range[1] + ay) % c.cc[1] + c.cc[1]) % c.cc[1];
+                    const int ncz = ((ic[2] - c.range[2] + az) % c.cc[2] + c.cc[2]) % c.cc[2];
+                    const int cell = ncx * c.cc[1] * c.cc[2] + ncy * c.cc[2] + ncz;
+                    const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
+                    const float dhx = m.dhi[code][0], dhy = m.dhi[code][1], dhz = m.dhi[code][2];
+                    const float dlx = m.dlo[code][0], dly = m.dlo[code][1], dlz = m.dlo[code][2];
+                    for (int kind = 0; kind < 2; ++kind) {
+                        const int off = kind ? c.tot : 0;
+                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                        for (int cb = b; cb < e; cb += 32) {
+                            const int t = cb + lane;
+                            bool keep = false;
+                            float4 pj, vj, lj;
+                            if (t < e) {
+                                ldg_pv(pv, t, pj, vj);
+                                lj = phl[2 * (size_t)t + 1];
+                                pj.x += dhx;  // exact: both on the hi grid
+                                pj.y += dhy;
+                                pj.z += dhz;
+                                const float ex = fmaxf(0.0f, fmaxf(b0x - pj.x, pj.x - b1x));
+                                const float ey = fmaxf(0.0f, fmaxf(b0y - pj.y, pj.y - b1y));
+                                const float ez = fmaxf(0.0f, fmaxf(b0z - pj.z, pj.z - b1z));
+                                keep = ex * ex + ey * ey + ez * ez < m.walk_r2;
+                            }
+                            const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                            if (keep) {
+                                const int slot = __popc(kept & ((1u << lane) - 1u));
+                                stage[slot].p = pj;
+                                stage[slot].v = vj;
+                                stage[slot].l = make_float4(lj.x + dlx, lj.y + dly, lj.z + dlz, __int_as_float(t));
+                                if (ST) gstage[slot] = gca[t];
+                            }
+                            __syncwarp();
+                            const int cnt = __popc(kept);
+                            if (act) {
+                                for (int q = 0; q < cnt; ++q) {
+                                    const float4 A = stage[q].p;
+                                    const float hx = A.x - pi.x, hy = A.y - pi.y, hz = A.z - pi.z;  // exact
+                                    const float r2h = hx * hx + hy * hy + hz * hz;
+                                    if (!(r2h < m.walk_r2)) continue;
+                                    const float4 L = stage[q].l;
+                                    const int j = __float_as_int(L.w);
+                                    if (j == i) continue;
+                                    const float4 V = stage[q].v;
+                                    const int tj = __float_as_int(A.w);
+                                    if (r2h < m.walk_short2) {
+                                        const float dx = hx + (L.x - li.x);
+                                        const float dy = hy + (L.y - li.y);
+                                        const float dz = hz + (L.z - li.z);
+                                        const float r2 = dx * dx + dy * dy + dz * dz;
+                                        if (!(r2 < m.rv2 || r2 < m.rp2 || (ST && (r2 < m.ra2 || r2 < m.rg2)))) continue;
+                                        const float rinv = rsqrt_nr(r2);
+                                        const float r = r2 * rinv;
+                                        float sc = 0.0f;
+                                        if (r2 < m.rp2) sc += (vi.w + V.w) * fmaf(m.p_b, r, m.p_a) * rinv;
+                                        if (r2 < m.rv2) {
+                                            const float mu = m.uniform_mu ? mu_u : m.visc_mu[ti][tj];
+                                            const float ud = (V.x - vi.x) * dx + (V.y - vi.y) * dy + (V.z - vi.z) * dz;
+                                            sc += mu * ud * fmaf(m.v_b, r, m.v_a) * (rinv * rinv * rinv);
+                                        }
+                                        float3 tt = make_float3(0.f, 0.f, 0.f);
+                                        if (ST) sc += st_terms<RATIO>(m, ti, tj, r2, r, rinv, dx, dy, dz, gi, gstage[q], ai, tt);
+                                        kahan_add(fx, cx, fmaf(sc, dx, tt.x));
+                                        kahan_add(fy, cy, fmaf(sc, dy, tt.y));
+                                        kahan_add(fz, cz, fmaf(sc, dz, tt.z));
+                                    } else {
+                                        const float rinv = rsqrtf(r2h);
+                                        float sc = 0.0f;
+                                        if (r2h < m.rv2) {
+                                            const float r = r2h * rinv;
+                                            const float mu = m.uniform_mu ? mu_u : m.visc_mu[ti][tj];
+                                            const float ud = (V.x - vi.x) * hx + (V.y - vi.y) * hy + (V.z - vi.z) * hz;
+                                            sc = mu * ud * fmaf(m.v_b, r, m.v_a) * (rinv * rinv * rinv);
+                                        }
+                                        if (ST) {
+                                            if (r2h < m.ra2 || r2h < m.rg2) {
+                                                float3 tt = make_float3(0.f, 0.f, 0.f);
+                                                sc += st_terms<RATIO>(m, ti, tj, r2h, r2h * rinv, rinv, hx, hy, hz, gi,
+                                                                      gstage[q], ai, tt);
+                                                gx += tt.x;
+                                                gy += tt.y;
+                                                gz += tt.z;
+                                            }
+                                        }
+                                        gx = fmaf(sc, hx, gx);
+                                        gy = fmaf(sc, hy, gy);
+                                        gz = fmaf(sc, hz, gz);
+                                    }
+                                }
+                            }
+                            __syncwarp();
+                        }
+                    }
+                }
+        if (!act) continue;
+        double F0 = ((double)fx - (double)cx) + (double)gx;
+        double F1 = ((double)fy - (double)cy) + (double)gy;
+        double F2 = ((double)fz - (double)cz) + (double)gz;
+        double4 v = vel[i];
+        const double mass = c.density[ti] * c.vol;
+        F0 += mass * c.gravity[0];
+        F1 += mass * c.gravity[1];
+        F2 += mass * c.gravity[2];
+        v.x += F0 / mass * c.dt;
+        v.y += F1 / mass * c.dt;
+        v.z += F2 / mass * c.dt;
+        if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
+        force[i] = make_double4(F0, F1, F2, 0.0);
+        vel_out[i] = v;
+    }
+}
+
 // DensityA over the whole list (output only, without surface tension).
 __global__ void k_mix_density_a(MixConst m, const float4* __restrict__ p32, const unsigned* __restrict__ list,
                                 const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
@@ -813,6 +1007,7 @@ struct MixedState {
     int max_neighbors = 0;
     bool exported = false;
     bool s64 = false;  // FP64 pressure core (MPH_MODE_MIXED_P64)
+    bool walk = false; // force sweep by cell walk (MPH_MIXED_CELL_WALK)
 };
 
 static void mfree(MixedState* m) {
@@ -928,11 +1123,27 @@ static void launch_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t 
 #undef MIX_B1
 }
 
+static void launch_b_walk(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
+    const int nb = (2 * c.tot + kWalkWarps - 1) / kWalkWarps;
+#define MIX_W(ST, RATIO)                                                                                      \
+    k_mix_b_walk<ST, RATIO><<<nb, 32 * kWalkWarps, 0, s>>>(m->mc, c, d.cellstart, m->phl, m->pv, m->gca,    \
+                                                          d.vel[d.vcur], d.vel[1 - d.vcur], d.force, d.scal)
+    if (m->mc.has_st) {
+        if (m->mc.ratio_all_one) { MIX_W(true, false); } else { MIX_W(true, true); }
+    } else {
+        if (m->mc.ratio_all_one) { MIX_W(false, false); } else { MIX_W(false, true); }
+    }
+#undef MIX_W
+}
+
 int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
-    launch_b<false>(m, c, d, s);
+    if (m->walk) launch_b_walk(m, c, d, s);
+    else launch_b<false>(m, c, d, s);
     m->exported = false;
     return 1;
 }
+
+void mixed_set_cell_walk(MixedState* m, bool on) { m->walk = on; }
 
 void mixed_move(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s) {
     k_mix_move<<<blocks(c.n, 256), 256, 0, s>>>(c, m->mc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.snap,
@@ -986,6 +1197,15 @@ int mixed_create(MixedState** out, const SimConst& c, const mph_constants& k, De
     const double rl = k.max_radius + margin, rs = k.radius_p + margin;
     mc.list_r2 = (float)(rl * rl);
     mc.short_r2 = (float)(rs * rs);
+    {
+        // the hi-only distance is within 3 * 1.5 grid steps of the exact one
+        // (the lo parts of both particles and of the cell offset): 8 steps of slack
+        double rf = std::max(c.rv, c.rp);
+        if (c.has_st) rf = std::max(rf, std::max(c.ra, c.rg));
+        const double sl = 8.0 * mc.grid;
+        mc.walk_r2 = (float)((rf + sl) * (rf + sl));
+        mc.walk_short2 = (float)((c.rp + sl) * (c.rp + sl));
+    }
     mc.ra2 = (float)c.ra2;
     mc.rp2 = (float)c.rp2;
     mc.rv2 = (float)c.rv2;

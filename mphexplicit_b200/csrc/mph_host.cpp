@@ -74,6 +74,7 @@ struct ReadBack {
 
 struct mph_ctx {
     int mode = MPH_MODE_FP64;
+    bool cell_walk = false;  // MPH_MIXED_CELL_WALK
     int n_fluid = 0;
     LearnedState lrn;
     int dim = 3;
@@ -606,6 +607,7 @@ static int create_impl(mph_ctx* ctx, const int* type, const double* xyz, const d
     // DensityP (main.cpp:358-364)
     if (ctx->mode == MPH_MODE_MIXED || ctx->mode == MPH_MODE_MIXED_P64) {
         TRY(mph::mixed_create(&ctx->mixed, ctx->sc, ctx->c, d, ctx->mode == MPH_MODE_MIXED_P64, st, &ctx->err));
+        mph::mixed_set_cell_walk(ctx->mixed, ctx->cell_walk);
     } else {
         TRY(grow_list(ctx, initial_capacity(ctx, ctx->sc.rm2)));
         if (uses_short_list(ctx)) {
@@ -626,8 +628,12 @@ extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim
     *out = nullptr;
     if (!p || !h || !type || !xyz || !vel) return fail(nullptr, MPH_ERR_ARG, "NULL argument");
     if (dim != 2 && dim != 3) return fail(nullptr, MPH_ERR_ARG, "dim must be 2 or 3");
+    const bool walk = (mode & MPH_MIXED_CELL_WALK) != 0;
+    mode &= ~MPH_MIXED_CELL_WALK;
     if (mode != MPH_MODE_FP64 && mode != MPH_MODE_MIXED && mode != MPH_MODE_MIXED_P64 && mode != MPH_MODE_LEARNED)
         return fail(nullptr, MPH_ERR_ARG, "unknown mode");
+    if (walk && mode != MPH_MODE_MIXED && mode != MPH_MODE_MIXED_P64)
+        return fail(nullptr, MPH_ERR_ARG, "MPH_MIXED_CELL_WALK applies to the mixed forms only");
     if (h->particle_count <= 0) return fail(nullptr, MPH_ERR_ARG, "particle_count must be > 0");
     if (!(p->dt > 0.0) || !std::isfinite(p->dt)) return fail(nullptr, MPH_ERR_ARG, "Dt must be finite and > 0");
     for (int d = 0; d < 3; ++d)
@@ -635,6 +641,7 @@ extern "C" int mph_create(const mph_params* p, const mph_grid_header* h, int dim
     TRY(validate_inputs(h->particle_count, type, xyz, vel));
     mph_ctx* ctx = new mph_ctx();
     ctx->mode = mode;
+    ctx->cell_walk = walk;
     for (int i = 0; i < h->particle_count; ++i) ctx->n_fluid += type[i] < 2 ? 1 : 0;
     ctx->dim = dim;
     ctx->n = h->particle_count;
@@ -1013,7 +1020,7 @@ extern "C" int mph_get_info(mph_ctx* ctx, mph_info* info) {
     info->step = ctx->step;
     info->rebuild_count = ctx->rebuilds;
     info->time = ctx->time;
-    info->mode = ctx->mode;
+    info->mode = ctx->mode | (ctx->cell_walk ? MPH_MIXED_CELL_WALK : 0);
     return MPH_OK;
 }
 

@@ -25,6 +25,8 @@ void mixed_sweep_a(MixedState* m, const SimConst& c, DevFP64& d, bool advance_wa
 // Force sweep (FP32 pairs) + FP64 velocity update into d.vel[1 - d.vcur];
 // returns the number of launches (1).
 int mixed_sweep_b(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s);
+// Force sweep by cell walk (no long table read) instead of the table sweep.
+void mixed_set_cell_walk(MixedState* m, bool on);
 // Fill the output-only fields (DensityA, wall forces, neighbour counts).
 int mixed_export(MixedState* m, const SimConst& c, DevFP64& d, cudaStream_t s, std::string* err, int* launches);
 // VirialPressureAtParticle into d.virial_p (FP32 pair terms, output only).

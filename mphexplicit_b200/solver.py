@@ -211,7 +211,9 @@ def compute_constants(params: N.Params, header: N.GridHeader, dim: int) -> N.Con
     return c
 
 
-_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED, "mixed_p64": N.MODE_MIXED_P64, "learned": N.MODE_LEARNED}
+_MODES = {"fp64": N.MODE_FP64, "mixed": N.MODE_MIXED, "mixed_p64": N.MODE_MIXED_P64, "learned": N.MODE_LEARNED,
+          # the mixed forms with the table-free (cell-walk) force sweep
+          "mixed_walk": N.MODE_MIXED | N.MIXED_CELL_WALK, "mixed_p64_walk": N.MODE_MIXED_P64 | N.MIXED_CELL_WALK}
 
 
 class Solver:

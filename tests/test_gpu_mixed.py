@@ -16,8 +16,10 @@ from tests.common import by_original_id, micro_cases, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-# relative L2 velocity error bounds after the given steps
-TOL = {"mixed": 1e-4, "mixed_p64": 1e-4}
+# relative L2 velocity error bounds after the given steps ("_walk": the same
+# form with the table-free cell-walk force sweep, MPH_MIXED_CELL_WALK)
+TOL = {"mixed": 1e-4, "mixed_p64": 1e-4, "mixed_walk": 1e-4, "mixed_p64_walk": 1e-4}
+MODES = list(TOL)
 
 
 def run(sc, steps, mode):
@@ -43,7 +45,7 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("mode", ["mixed", "mixed_p64"])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("name,make,steps", CASES)
 def test_mixed_error_against_fp64(name, make, steps, mode):
     sc = make()
@@ -67,7 +69,7 @@ def test_mixed_error_against_fp64(name, make, steps, mode):
 def test_mixed_momentum_free_droplet():
     """No walls, no gravity: total momentum stays at its initial zero."""
     sc = scenes.droplet_2d(seed=8)
-    for mode in ("mixed", "mixed_p64"):
+    for mode in MODES:
         _, _, cons = run(sc, 500, mode)
         mass = cons[0]
         assert np.all(np.abs(cons[1:3]) < 1e-7 * mass), (mode, cons)
@@ -79,13 +81,13 @@ def test_mixed_full_size_dam_break_1000_steps():
     reference) after 1000 steps."""
     sc = scenes.dam_break_3d()
     ref, _, _ = run(sc, 1000, "fp64")
-    for mode in ("mixed", "mixed_p64"):
+    for mode in MODES:
         got, _, _ = run(sc, 1000, mode)
         err = vel_error(ref, got)
         assert err <= 1e-4, (mode, err)
 
 
-@pytest.mark.parametrize("mode", ["mixed", "mixed_p64"])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("k", range(6))
 def test_mixed_micro_cases(k, mode):
     """The micro-cases (pairs at every radius, a lone particle, an isolated
@@ -97,6 +99,18 @@ def test_mixed_micro_cases(k, mode):
     assert err <= TOL[mode], f"{name} {mode}: {err:.3e}"
     assert rel_l2(by_original_id(got, "xyz"), by_original_id(ref, "xyz")) < 1e-6
     assert np.array_equal(by_original_id(got, "neighbor_count"), by_original_id(ref, "neighbor_count"))
+
+
+@pytest.mark.parametrize("name,make,steps", CASES)
+def test_cell_walk_matches_table_sweep(name, make, steps):
+    """The cell-walk force sweep evaluates the same pair terms as the table
+    sweep: after a few steps the two mixed runs agree far inside the form's
+    bound (they differ only in FP32 summation order and in which pairs take
+    the exact hi/lo displacement)."""
+    sc = make()
+    a, _, _ = run(sc, 20, "mixed")
+    b, _, _ = run(sc, 20, "mixed_walk")
+    assert vel_error(a, b) < 1e-5, vel_error(a, b)
 
 
 @pytest.mark.parametrize("mode", ["mixed", "mixed_p64"])

@@ -245,3 +245,20 @@ def test_checkpoint_file_round_trip_is_exact_and_rejects_bad_files():
             M.read_checkpoint(path)
         with pytest.raises(M.MphError):
             M.read_checkpoint(os.path.join(td, "missing.ckpt"))
+
+
+def test_create_rejects_bad_modes_before_any_device_call():
+    """mph_create checks its mode before it touches the device: an unknown
+    mode, and the cell-walk flag on a form other than the mixed ones."""
+    import ctypes as C
+    lib = N.load()
+    sc = scenes.dam_break_3d(fluid=(6, 5, 7), box=(14, 6, 12))
+    t = np.ascontiguousarray(sc.type, np.int32)
+    x = np.ascontiguousarray(sc.xyz, np.float64)
+    v = np.ascontiguousarray(sc.vel, np.float64)
+    for mode in (7, N.MODE_FP64 | N.MIXED_CELL_WALK, N.MODE_LEARNED | N.MIXED_CELL_WALK):
+        ctx = C.c_void_p()
+        rc = lib.mph_create(C.byref(sc.params), C.byref(sc.header), 3, mode, t.ctypes.data_as(C.POINTER(C.c_int)),
+                            x.ctypes.data_as(C.POINTER(C.c_double)), v.ctypes.data_as(C.POINTER(C.c_double)),
+                            C.byref(ctx))
+        assert rc == N.MPH_ERR_ARG and not ctx.value, mode
