@@ -172,7 +172,10 @@ __global__ void k_reorder(int n, const int* __restrict__ vals, const int* __rest
 // neighbouring cell's), which only keeps more candidates.
 constexpr int kListWarps = 4;  // warps (home keys) per 128-thread block
 
-__global__ void __launch_bounds__(32 * kListWarps, 6)
+#ifndef MPH_LIST_MINB
+#define MPH_LIST_MINB 6
+#endif
+__global__ void __launch_bounds__(32 * kListWarps, MPH_LIST_MINB)
 k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __restrict__ pos32, Prefilter pf,
                 const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist, int cap,
                 int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s, StepScalars* __restrict__ scal) {
@@ -205,6 +208,7 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
     const size_t n = (size_t)c.n;
     const bool short_list = nlist_s != nullptr;
     float4* cw = cand[wib];
+    const float kInf = __int_as_float(0x7f800000);
     for (int h0 = hb; h0 < he; h0 += 32) {
         const int i = h0 + lane;
         const bool active = i < he;
@@ -212,6 +216,18 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
         const float4 fi = pos32[active ? i : hb];
         const bool is_wall = wall_begin <= i && i < wall_end;
         int cnt = 0, cnt_s = 0;
+        // box of the chunk's FP32 positions: a candidate farther than the
+        // cut-off from it is no lane's neighbour (Prefilter::r2_box)
+        float b0x = active ? fi.x : kInf, b0y = active ? fi.y : kInf, b0z = active ? fi.z : kInf;
+        float b1x = active ? fi.x : -kInf, b1y = active ? fi.y : -kInf, b1z = active ? fi.z : -kInf;
+        for (int o = 16; o > 0; o >>= 1) {
+            b0x = fminf(b0x, __shfl_xor_sync(0xffffffffu, b0x, o));
+            b0y = fminf(b0y, __shfl_xor_sync(0xffffffffu, b0y, o));
+            b0z = fminf(b0z, __shfl_xor_sync(0xffffffffu, b0z, o));
+            b1x = fmaxf(b1x, __shfl_xor_sync(0xffffffffu, b1x, o));
+            b1y = fmaxf(b1y, __shfl_xor_sync(0xffffffffu, b1y, o));
+            b1z = fmaxf(b1z, __shfl_xor_sync(0xffffffffu, b1z, o));
+        }
         for (int kind = 0; kind < 2; ++kind) {
             // main.cpp:1416: a wall with no fluid neighbour gets no wall entries
             const bool take = active && !(kind == 1 && is_wall && cnt == 0);
@@ -228,33 +244,65 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
                         const float oz = pf.use[2] ? gz - fi.z : 0.f;
                         const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
                         for (int cb = b; cb < e; cb += 32) {
-                            const int m = min(32, e - cb);
+                            // the candidates near the box, compacted in order into the stage
+                            bool near = false;
+                            float4 q;
+                            if (cb + lane < e) {
+                                q = pos32[cb + lane];
+                                const float ax = q.x + gx, ay = q.y + gy, az = q.z + gz;
+                                const float ex = pf.use[0] ? fmaxf(0.f, fmaxf(b0x - ax, ax - b1x)) : 0.f;
+                                const float ey = pf.use[1] ? fmaxf(0.f, fmaxf(b0y - ay, ay - b1y)) : 0.f;
+                                const float ez = pf.use[2] ? fmaxf(0.f, fmaxf(b0z - az, az - b1z)) : 0.f;
+                                near = ex * ex + ey * ey + ez * ez <= pf.r2_box;
+                            }
+                            const unsigned kept = __ballot_sync(0xffffffffu, near);
                             __syncwarp();
-                            if (lane < m) cw[lane] = pos32[cb + lane];
+                            if (near) {
+                                q.w = __int_as_float(lane);
+                                cw[__popc(kept & ((1u << lane) - 1u))] = q;
+                            }
                             __syncwarp();
-                            unsigned mask = 0u;
+                            const int m = __popc(kept);
+                            // per candidate of the stage: may be within rm (mask), needs the
+                            // FP64 test (exact: in a shell of the rm or the rs bound), within
+                            // rs for certain (in_s)
+                            unsigned mask = 0u, exact = 0u, in_s = 0u;
                             if (take) {
                                 for (int t = 0; t < m; ++t) {
                                     const float4 q = cw[t];
                                     const float fx = pf.use[0] ? q.x + ox : 0.f;
                                     const float fy = pf.use[1] ? q.y + oy : 0.f;
                                     const float fz = pf.use[2] ? q.z + oz : 0.f;
-                                    if (fx * fx + fy * fy + fz * fz <= pf.r2_hi) mask |= 1u << t;
+                                    const float r2f = fx * fx + fy * fy + fz * fz;
+                                    if (r2f <= pf.r2_hi) {
+                                        const unsigned bit = 1u << t;
+                                        mask |= bit;
+                                        if (r2f > pf.r2_lo || (short_list && r2f > pf.rs2_lo && r2f <= pf.rs2_hi))
+                                            exact |= bit;
+                                        else if (r2f <= pf.rs2_lo)
+                                            in_s |= bit;
+                                    }
                                 }
                             }
                             while (mask) {
                                 const int t = __ffs(mask) - 1;
+                                const unsigned bit = mask & (0u - mask);
                                 mask &= mask - 1u;
-                                const int j = cb + t;
-                                const double4 pj = pos[j];
-                                const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-                                const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-                                const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
-                                const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-                                if (r2 <= c.rm2) {
+                                const int j = cb + __float_as_int(cw[t].w);
+                                bool in = true, in_short = (in_s & bit) != 0u;
+                                if (exact & bit) {
+                                    const double4 pj = pos[j];
+                                    const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+                                    const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+                                    const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+                                    const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                                    in = r2 <= c.rm2;
+                                    in_short = r2 <= c.rs2;
+                                }
+                                if (in) {
                                     if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
                                     cnt++;
-                                    if (short_list && r2 <= c.rs2) {
+                                    if (short_list && in_short) {
                                         if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
                                         cnt_s++;
                                     }
@@ -363,6 +411,12 @@ void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, cons
 // 1 + 2^-21 of its exact value: a candidate the FP64 test accepts (r <= rm)
 // has an FP32 distance squared below (rm + 2e)^2 (1 + 2^-20), rounded up to
 // the next float.  e is taken as 8 * 2^-24 * W for room.
+// The box test of a candidate (its image q + offset against the box of the
+// FP32 positions of the warp's particles) bounds each axis' gap by the
+// component for every particle in the box, within the same e (the image sum
+// q + offset rounds once, within 2^-24 2W): a candidate within rm of any of
+// them has a box distance squared below (rm + 2e)^2 (1 + 2^-20); r2_box takes
+// 4e for room.
 Prefilter make_prefilter(const SimConst& c) {
     Prefilter pf{};
     double wmax = 0.0;
@@ -375,6 +429,29 @@ Prefilter make_prefilter(const SimConst& c) {
     const double rm = std::sqrt(c.rm2);
     const double t = (rm + 2.0 * e) * (rm + 2.0 * e) * (1.0 + std::ldexp(1.0, -20));
     pf.r2_hi = std::nextafter((float)t, 3.0e38f);
+    const double tb = (rm + 4.0 * e) * (rm + 4.0 * e) * (1.0 + std::ldexp(1.0, -20));
+    pf.r2_box = std::nextafter((float)tb, 3.0e38f);
+    // The other side of the same bounds: an FP32 distance squared at or below
+    // (R - 2e)^2 (1 - 2^-20), rounded down to the previous float, puts the FP64
+    // distance below R - 2e + 2e = R, so the FP64 test r2 <= R^2 holds for
+    // certain and is skipped; only the candidates in the shell between the two
+    // bounds take it.  Valid when every axis is compared in FP32 (an axis left
+    // out of the prefilter contributes 0 in FP32 but not in FP64), or the axis
+    // left out is the flat one of a 2-D run.
+    bool all_axes = true;
+    for (int d = 0; d < 3; ++d)
+        if (!pf.use[d] && !(c.dim == 2 && d == 2)) all_axes = false;
+    auto lo_bound = [&](double r) {
+        if (!all_axes || r <= 2.0 * e) return -1.0f;
+        const double t2 = (r - 2.0 * e) * (r - 2.0 * e) * (1.0 - std::ldexp(1.0, -20));
+        return std::nextafter((float)t2, -1.0f);
+    };
+    const double rs = std::sqrt(c.rs2);
+    pf.r2_lo = lo_bound(rm);
+    pf.rs2_lo = lo_bound(rs);
+    pf.rs2_hi = all_axes ? std::nextafter((float)((rs + 2.0 * e) * (rs + 2.0 * e) * (1.0 + std::ldexp(1.0, -20))),
+                                          3.0e38f)
+                         : 3.0e38f;
     return pf;
 }
 

@@ -305,37 +305,6 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
 // their order in each sum are the reference's; the main loop no longer runs
 // the pressure block under a branch that some lane takes on nearly every
 // entry while most lanes wait.
-// Row i of an [n][3] FP64 array in pinned host memory mapped into the device
-// (the velocity read-back of mph_step_read_state).  When the 32 lanes of the
-// warp are here together with consecutive rows (an even first row, so the
-// warp's 768 bytes start on a 16-byte boundary of a 16-byte aligned array),
-// the rows go through the warp's 96-double stage in shared memory and out as
-// 16-byte stores covering whole 128-byte lines: full-line writes over PCIe
-// instead of 8-byte pieces.  Otherwise each lane stores its own three values.
-__device__ __forceinline__ void store_host_row3(double* __restrict__ out, int i, double x, double y, double z,
-                                                double* __restrict__ stage) {
-    const unsigned m = __activemask();
-    const int lane = threadIdx.x & 31;
-    if (m == 0xffffffffu) {
-        const int first = __shfl_sync(m, i, 0);
-        if (__all_sync(m, i == first + lane) && (first & 1) == 0) {
-            stage[3 * lane] = x;
-            stage[3 * lane + 1] = y;
-            stage[3 * lane + 2] = z;
-            __syncwarp(m);
-            double2* dst = reinterpret_cast<double2*>(out + 3 * (size_t)first);
-            const double2* src = reinterpret_cast<const double2*>(stage);
-            dst[lane] = src[lane];
-            if (lane < 16) dst[32 + lane] = src[32 + lane];
-            __syncwarp(m);
-            return;
-        }
-    }
-    out[3 * (size_t)i] = x;
-    out[3 * (size_t)i + 1] = y;
-    out[3 * (size_t)i + 2] = z;
-}
-
 template <bool ST, bool RATIO, bool LRN, bool SPLIT>
 __global__ void __launch_bounds__(128, MPH_SWEEPB_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
@@ -344,8 +313,6 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
           const int* __restrict__ nlist_s, double4* __restrict__ force,
           StepScalars* __restrict__ scal, const int* __restrict__ eoff, const float4* __restrict__ eforce,
           float4* __restrict__ lsum, int part, int i0, int i1, double* __restrict__ vel_host) {
-    __shared__ __align__(16) double vstage[4][96];  // store_host_row3, one stage per warp
-    double* const stage = vstage[threadIdx.x >> 5];
     const int i = i0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);  // particles [i0, i1)
     if (i >= i1) return;
     const int nf = cellstart[c.tot];
@@ -354,7 +321,11 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     // writes for it) and its force is left for part 2 (output only)
     if (part == 1 && i >= nf) {
         vel_out[i] = make_double4(vi.x, vi.y, vi.z, 0.0);
-        if (vel_host) store_host_row3(vel_host, i, vi.x, vi.y, vi.z, stage);
+        if (vel_host) {
+            vel_host[3 * (size_t)i] = vi.x;
+            vel_host[3 * (size_t)i + 1] = vi.y;
+            vel_host[3 * (size_t)i + 2] = vi.z;
+        }
         return;
     }
     if (part == 2 && i < nf) return;
@@ -530,8 +501,11 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     force[i] = make_double4(F0, F1, F2, 0.0);
     if (part != 2) {
         vel_out[i] = vn;
-        // mapped pinned host memory: the read-back travels while the sweep runs
-        if (vel_host) store_host_row3(vel_host, i, vn.x, vn.y, vn.z, stage);
+        if (vel_host) {  // mapped pinned host memory: the read-back travels while the sweep runs
+            vel_host[3 * (size_t)i] = vn.x;
+            vel_host[3 * (size_t)i + 1] = vn.y;
+            vel_host[3 * (size_t)i + 2] = vn.z;
+        }
     }
 }
 

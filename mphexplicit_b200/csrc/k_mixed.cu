@@ -236,11 +236,25 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
     const size_t n = (size_t)c.n;
     const int cap_s = m.cap_s;
     float4* cw = cand[wib];
+    const float kInf = __int_as_float(0x7f800000);
     for (int h0 = hb; h0 < he; h0 += 32) {
         const int i = h0 + lane;
         const bool active = i < he;
         const float4 pi = p32[active ? i : hb];
         const bool is_wall = i >= nf;
+        // box of the chunk's hi positions: the hi values, the cell offsets and
+        // their sums and differences are exact on the hi grid, so a candidate
+        // whose distance to the box is beyond the cut-off is no lane's neighbour
+        float b0x = active ? pi.x : kInf, b0y = active ? pi.y : kInf, b0z = active ? pi.z : kInf;
+        float b1x = active ? pi.x : -kInf, b1y = active ? pi.y : -kInf, b1z = active ? pi.z : -kInf;
+        for (int o = 16; o > 0; o >>= 1) {
+            b0x = fminf(b0x, __shfl_xor_sync(0xffffffffu, b0x, o));
+            b0y = fminf(b0y, __shfl_xor_sync(0xffffffffu, b0y, o));
+            b0z = fminf(b0z, __shfl_xor_sync(0xffffffffu, b0z, o));
+            b1x = fmaxf(b1x, __shfl_xor_sync(0xffffffffu, b1x, o));
+            b1y = fmaxf(b1y, __shfl_xor_sync(0xffffffffu, b1y, o));
+            b1z = fmaxf(b1z, __shfl_xor_sync(0xffffffffu, b1z, o));
+        }
         uint4* const ls = reinterpret_cast<uint4*>(list) + i;
         uint4* const ll = reinterpret_cast<uint4*>(list) + (size_t)(cap_s >> 2) * n + i;
         int cs = 0, cl = 0;
@@ -272,14 +286,29 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
                         const int off = kind ? c.tot : 0;
                         const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
                         for (int cb = b; cb < e; cb += 32) {
-                            const int mm = min(32, e - cb);
+                            bool near = false;
+                            float4 qc;
+                            if (cb + lane < e) {
+                                qc = p32[cb + lane];
+                                const float ax = qc.x + m.dhi[code][0], ay = qc.y + m.dhi[code][1],
+                                            az = qc.z + m.dhi[code][2];
+                                const float ex = fmaxf(0.f, fmaxf(b0x - ax, ax - b1x));
+                                const float ey = fmaxf(0.f, fmaxf(b0y - ay, ay - b1y));
+                                const float ez = fmaxf(0.f, fmaxf(b0z - az, az - b1z));
+                                near = ex * ex + ey * ey + ez * ez < m.list_r2;
+                            }
+                            const unsigned kept = __ballot_sync(0xffffffffu, near);
                             __syncwarp();
-                            if (lane < mm) cw[lane] = p32[cb + lane];
+                            if (near) {
+                                qc.w = __int_as_float(cb + lane);
+                                cw[__popc(kept & ((1u << lane) - 1u))] = qc;
+                            }
                             __syncwarp();
                             if (!active) continue;
+                            const int mm = __popc(kept);
                             for (int t = 0; t < mm; ++t) {
-                                const int j = cb + t;
                                 const float4 q = cw[t];
+                                const int j = __float_as_int(q.w);
                                 const float dx = q.x + ox, dy = q.y + oy, dz = q.z + oz;
                                 const float r2 = dx * dx + dy * dy + dz * dz;
                                 if (r2 < m.list_r2 && j != i) {

@@ -1087,7 +1087,6 @@ static double* mapped_host(double* p, size_t count) {
     if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
         return nullptr;
     if ((char*)b.devicePointer - (char*)a.devicePointer != (ptrdiff_t)((count - 1) * sizeof(double))) return nullptr;
-    if (((uintptr_t)a.devicePointer & 15u) != 0) return nullptr;  // the sweep's 16-byte stores
     return (double*)a.devicePointer;
 }
 

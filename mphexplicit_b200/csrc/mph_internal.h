@@ -114,7 +114,10 @@ void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, cons
 struct Prefilter {
     int use[3];
     float width[3];
-    float r2_hi;
+    float r2_hi;   // per pair: FP32 distance squared at or below it for every pair within rm
+    float r2_box;  // per candidate: FP32 distance squared to the box around a warp's particles
+    float r2_lo;   // FP32 distance squared at or below it: within rm in FP64 for certain (-1: never)
+    float rs2_lo, rs2_hi;  // the same two bounds for the short radius rs
 };
 Prefilter make_prefilter(const SimConst& c);
 // FP32 positions relative to the domain origin (the prefilter's input).
