@@ -175,6 +175,7 @@ constexpr int kListWarps = 4;  // warps (home keys) per 128-thread block
 #ifndef MPH_LIST_MINB
 #define MPH_LIST_MINB 6
 #endif
+template <bool ALL3>  // every axis in the FP32 prefilter (pf.use all set)
 __global__ void __launch_bounds__(32 * kListWarps, MPH_LIST_MINB)
 k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __restrict__ pos32, Prefilter pf,
                 const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist, int cap,
@@ -239,9 +240,9 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
                         const int cx = slot(0, jx % w[0], gx), cy = slot(1, jy % w[1], gy),
                                   cz = slot(2, jz % w[2], gz);
                         const int cell = cell_id(c, cx, cy, cz);
-                        const float ox = pf.use[0] ? gx - fi.x : 0.f;
-                        const float oy = pf.use[1] ? gy - fi.y : 0.f;
-                        const float oz = pf.use[2] ? gz - fi.z : 0.f;
+                        const float ox = (ALL3 || pf.use[0]) ? gx - fi.x : 0.f;
+                        const float oy = (ALL3 || pf.use[1]) ? gy - fi.y : 0.f;
+                        const float oz = (ALL3 || pf.use[2]) ? gz - fi.z : 0.f;
                         const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
                         for (int cb = b; cb < e; cb += 32) {
                             // the candidates near the box, compacted in order into the stage
@@ -250,10 +251,10 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
                             if (cb + lane < e) {
                                 q = pos32[cb + lane];
                                 const float ax = q.x + gx, ay = q.y + gy, az = q.z + gz;
-                                const float ex = pf.use[0] ? fmaxf(0.f, fmaxf(b0x - ax, ax - b1x)) : 0.f;
-                                const float ey = pf.use[1] ? fmaxf(0.f, fmaxf(b0y - ay, ay - b1y)) : 0.f;
-                                const float ez = pf.use[2] ? fmaxf(0.f, fmaxf(b0z - az, az - b1z)) : 0.f;
-                                near = ex * ex + ey * ey + ez * ez <= pf.r2_box;
+                                const float ex = (ALL3 || pf.use[0]) ? fmaxf(0.f, fmaxf(b0x - ax, ax - b1x)) : 0.f;
+                                const float ey = (ALL3 || pf.use[1]) ? fmaxf(0.f, fmaxf(b0y - ay, ay - b1y)) : 0.f;
+                                const float ez = (ALL3 || pf.use[2]) ? fmaxf(0.f, fmaxf(b0z - az, az - b1z)) : 0.f;
+                                near = __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, __fmul_rn(ez, ez))) <= pf.r2_box;
                             }
                             const unsigned kept = __ballot_sync(0xffffffffu, near);
                             __syncwarp();
@@ -270,10 +271,11 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
                             if (take) {
                                 for (int t = 0; t < m; ++t) {
                                     const float4 q = cw[t];
-                                    const float fx = pf.use[0] ? q.x + ox : 0.f;
-                                    const float fy = pf.use[1] ? q.y + oy : 0.f;
-                                    const float fz = pf.use[2] ? q.z + oz : 0.f;
-                                    const float r2f = fx * fx + fy * fy + fz * fz;
+                                    const float fx = (ALL3 || pf.use[0]) ? q.x + ox : 0.f;
+                                    const float fy = (ALL3 || pf.use[1]) ? q.y + oy : 0.f;
+                                    const float fz = (ALL3 || pf.use[2]) ? q.z + oz : 0.f;
+                                    // FMA: fewer roundings than the bound allows for
+                                    const float r2f = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, __fmul_rn(fz, fz)));
                                     if (r2f <= pf.r2_hi) {
                                         const unsigned bit = 1u << t;
                                         mask |= bit;
@@ -407,8 +409,9 @@ void launch_reorder(const SimConst& c, const int* vals, const int* pidx_in, cons
 // component is within e = 5 * 2^-24 * W of the FP64 minimum-image
 // displacement (W rounded to FP32 for the offset adds 2^-24 W), which is
 // itself within 2^-50 W of the true one.  The FP32 distance is then within
-// sqrt(3) e < 2e of the FP64 one, and the FP32 sum of squares within a factor
-// 1 + 2^-21 of its exact value: a candidate the FP64 test accepts (r <= rm)
+// sqrt(3) e < 2e of the FP64 one, and the FP32 sum of squares (three
+// roundings: a product and two FMAs) within a factor 1 + 2^-21 of its exact
+// value: a candidate the FP64 test accepts (r <= rm)
 // has an FP32 distance squared below (rm + 2e)^2 (1 + 2^-20), rounded up to
 // the next float.  e is taken as 8 * 2^-24 * W for room.
 // The box test of a candidate (its image q + offset against the box of the
@@ -463,8 +466,14 @@ void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* p
                           int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
                           StepScalars* scal, cudaStream_t s) {
     const long long keys = 2LL * c.tot;
-    k_neighbor_list<<<(int)((keys + kListWarps - 1) / kListWarps), 32 * kListWarps, 0, s>>>(
-        c, pos, pos32, make_prefilter(c), cellstart, ncount, nlist, cap, ncount_s, nlist_s, cap_s, scal);
+    const Prefilter pf = make_prefilter(c);
+    const int nb = (int)((keys + kListWarps - 1) / kListWarps);
+    if (pf.use[0] && pf.use[1] && pf.use[2])
+        k_neighbor_list<true><<<nb, 32 * kListWarps, 0, s>>>(c, pos, pos32, pf, cellstart, ncount, nlist, cap,
+                                                              ncount_s, nlist_s, cap_s, scal);
+    else
+        k_neighbor_list<false><<<nb, 32 * kListWarps, 0, s>>>(c, pos, pos32, pf, cellstart, ncount, nlist, cap,
+                                                               ncount_s, nlist_s, cap_s, scal);
 }
 
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s) {
