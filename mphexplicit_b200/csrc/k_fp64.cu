@@ -28,6 +28,17 @@
 #ifndef MPH_SWEEPB_MINB
 #define MPH_SWEEPB_MINB 5
 #endif
+// The surface-tension variants hold more live values per pair; at the
+// bounds above they spilled (140 B in the force sweep) and ran the 8.5 M
+// particle two-fluid column's step at 40.6 + 13.9 ms.  Measured on that
+// column: the force sweep 26.7 ms at 4 blocks (no spills) and 29.6 ms at 3,
+// sweep A 12.5 ms at 5 (13.3 at 6); results bit-identical.
+#ifndef MPH_SWEEP_MINB_ST
+#define MPH_SWEEP_MINB_ST 5
+#endif
+#ifndef MPH_SWEEPB_MINB_ST
+#define MPH_SWEEPB_MINB_ST 4
+#endif
 
 namespace mph {
 
@@ -164,7 +175,7 @@ __device__ __forceinline__ double s_dwv(const SimConst& c, double q) { return c.
 // when they are read, and visits only the short sublist (the pairs that can
 // lie within RadiusP, in list order).
 template <bool ST, bool RATIO, bool DA>
-__global__ void __launch_bounds__(128, MPH_SWEEP_MINB)
+__global__ void __launch_bounds__(128, ST ? MPH_SWEEP_MINB_ST : MPH_SWEEP_MINB)
 k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
           const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
           double* __restrict__ strain_p, double* __restrict__ div_p, double4* __restrict__ velp,
@@ -306,7 +317,7 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
 // the pressure block under a branch that some lane takes on nearly every
 // entry while most lanes wait.
 template <bool ST, bool RATIO, bool LRN, bool SPLIT>
-__global__ void __launch_bounds__(128, MPH_SWEEPB_MINB)
+__global__ void __launch_bounds__(128, ST ? MPH_SWEEPB_MINB_ST : MPH_SWEEPB_MINB)
 k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
           const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
           const int* __restrict__ ncount, const int* __restrict__ nlist, const int* __restrict__ ncount_s,
