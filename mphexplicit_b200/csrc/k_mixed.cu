@@ -34,6 +34,12 @@ constexpr int kCodeBits = 5;  // 27 neighbour-cell offsets
 #ifndef MPH_MIXB_MINB_FUSED
 #define MPH_MIXB_MINB_FUSED 8
 #endif
+// ... and of its surface-tension variants (more live values per pair): on the
+// 8.5 M-particle two-fluid column 10.06 ms at 8 blocks (some spilling), 10.28
+// at 6 and 11.06 at 5, results identical.
+#ifndef MPH_MIXB_MINB_ST
+#define MPH_MIXB_MINB_ST 8
+#endif
 // Resident 128-thread blocks per SM of the table-free force sweep.
 #ifndef MPH_WALK_MINB
 #define MPH_WALK_MINB 6
@@ -592,7 +598,7 @@ k_mix_a(MixConst m, const float4* __restrict__ phl, const float4* __restrict__ v
 // plain FP32 sum.  Then gravity and the FP64 velocity update
 // (main.cpp:1908-2010).
 template <bool ST, bool RATIO, bool WALLS>
-__global__ void __launch_bounds__(128, MPH_MIXB_MINB_FUSED)
+__global__ void __launch_bounds__(128, ST ? MPH_MIXB_MINB_ST : MPH_MIXB_MINB_FUSED)
 k_mix_b(MixConst m, SimConst c, const int* __restrict__ cellstart, const float4* __restrict__ phl,
         const float4* __restrict__ pv, const float4* __restrict__ gca,
         const unsigned* __restrict__ list, const int* __restrict__ cnt_short, const int* __restrict__ cnt_all,
