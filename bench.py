@@ -108,29 +108,74 @@ def ncu_pipe(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """SM clocks and clock-event (throttle) reasons during a timed region: the
+    recipe's `nvidia-smi -lms 200` line, started before the region (the
+    region waits for its first sample) and stopped after one more sample, plus
+    NVML read every 10 ms from a thread while the region runs (a region of a
+    few tens of ms falls between two nvidia-smi samples).  Reading clocks
+    changes nothing on the GPU."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
         self.path = tempfile.mktemp(suffix=".csv")
+        self.nvml = []  # (sm MHz, max sm MHz, reason names)
+        self._stop = None
+        self._thread = None
+
+    def _rows(self):
+        try:
+            return [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return []
+
+    def _nvml_loop(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.idx)
+            bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while True:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.nvml.append((float(sm), float(mx), [self.NAMES[k] for k in range(4) if r & bits[k]]))
+                if self._stop.wait(0.01):
+                    break
+            nv.nvmlShutdown()
+        except Exception:
+            pass
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "--id=%d" % self.idx, "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        time.sleep(0.3)
+        t0 = time.time()
+        while self.proc is not None and not self._rows() and time.time() - t0 < 10.0:
+            time.sleep(0.05)
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
+        self._thread.start()
+        time.sleep(0.02)
         return self
 
     def __exit__(self, *a):
+        self._stop.set()
+        self._thread.join(timeout=5)
         if self.proc:
+            n0, t0 = len(self._rows()), time.time()
+            while len(self._rows()) <= n0 and time.time() - t0 < 2.0:
+                time.sleep(0.05)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -138,19 +183,20 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
-        except Exception:
-            rows = []
-        if not rows:
+        rows = self._rows()
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        reasons = {self.NAMES[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                   and "Not" not in r[5 + k]}
+        for _, _, rs in self.nvml:
+            reasons.update(rs)
+        nv_sm = [x[0] for x in self.nvml]
+        if not sm and not nv_sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
-                          and "Not" not in r[5 + k]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        allsm = nv_sm if nv_sm else sm
+        return {"sm_mhz": float(np.median(allsm)), "sm_max_mhz": max(mx + [x[1] for x in self.nvml]) if (mx or nv_sm)
+                else None, "reasons": sorted(reasons), "samples": len(rows), "nvml_samples": len(nv_sm),
+                "sm_mhz_nvidia_smi": float(np.median(sm)) if sm else None}
 
 
 # edge-MLP flops per evaluated edge: 2 * (9*128 + 128*128 + 128*128 + 128*3)
