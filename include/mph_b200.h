@@ -396,15 +396,14 @@ int mph_check_exact_division(long long n, unsigned long long seed, long long* mi
  * stream is a cudaStream_t (NULL: the legacy default stream) and the call is
  * asynchronous on it.  The sort's scratch is a fixed static device array of
  * 2^21 ints (8 MiB), so n must be below 2^20 (1,048,576); larger n returns
- * MPH_ERR_CAPACITY.  The first call on a device is its set-up: it looks up
- * that array's device address (once per device for the life of the process),
- * and under CUDA's lazy module loading (the default) it is also the call that
- * loads the library's module, and with it the 8 MiB array, onto that device,
- * which then holds it until the process exits.  Callers with a fixed device
- * budget should therefore make the first call during their own set-up, and
- * before any stream capture.  A process that resets a device
- * (cudaDeviceReset) must not call this entry point on it again: the address
- * looked up at set-up belongs to the context that was reset.  All calls share the one
+ * MPH_ERR_CAPACITY.  Each call looks up that array's device address in the
+ * current context (no allocation once the module is loaded); under CUDA's
+ * lazy module loading (the default) the first call on a device, or the first
+ * after a device reset, is the one that loads the library's module, and with
+ * it the 8 MiB array, onto that device, which then holds it until the process
+ * exits (or the next reset).  Callers with a fixed device budget should
+ * therefore make the first call during their own set-up, and before any
+ * stream capture.  All calls share the one
  * scratch array: calls that overlap on the GPU (other streams, other host
  * threads) race and must be serialised by the caller.  Allocates nothing
  * (no cudaMalloc, cudaFree or allocating library call). */

@@ -9,7 +9,6 @@
 // padded to a power of two) lives in the file-scope array below instead of
 // memory the library would allocate.
 #include <cstring>
-#include <mutex>
 #include <string>
 #include "mph_internal.h"
 
@@ -22,27 +21,18 @@ namespace {
 constexpr int kNoAllocMaxPow2 = 1 << 20;
 __device__ __align__(256) int g_sort_scratch[2 * kNoAllocMaxPow2];
 
-// Device address of g_sort_scratch per device, looked up once with that device
-// current (the array's name in host code is only a host-side stand-in).
-std::mutex g_scratch_mu;
-constexpr int kMaxDevices = 64;
-int* g_scratch_ptr[kMaxDevices] = {};
-
+// Device address of g_sort_scratch in the current context, looked up on
+// every call (the array's name in host code is only a host-side stand-in).
+// Once the module is loaded the lookup allocates nothing; not caching it
+// keeps the address right after a device reset or with another context
+// current on the same device.
 int scratch_on_current_device(int** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return set_thread_error(MPH_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices) return set_thread_error(MPH_ERR_CUDA, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_sort_scratch);
-        if (e != cudaSuccess || !p)
-            return set_thread_error(MPH_ERR_CUDA,
-                                    std::string("cudaGetSymbolAddress(sort scratch): ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<int*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_sort_scratch);
+    if (e != cudaSuccess || !p)
+        return set_thread_error(MPH_ERR_CUDA,
+                                std::string("cudaGetSymbolAddress(sort scratch): ") + cudaGetErrorString(e));
+    *out = static_cast<int*>(p);
     return MPH_OK;
 }
 
