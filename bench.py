@@ -404,6 +404,62 @@ def measure_batch(args, rank):
     return out
 
 
+def measure_droplet(args, rank):
+    """Benchmark config 1: the 2-D square droplet (40x40 type-0 particles,
+    l0 = 0.004 m, mu 0.1, sigma 0.07, sound speed 10 m/s, dt 1e-5 s, no walls or
+    gravity), FP64, `droplet_steps` steps in one mph_step call: graph launches
+    (the default for several FP64 steps) against the host path (one flag read
+    per step), both bit-identical, and the reference's own 2-D build on the
+    same scene on all host threads and on one."""
+    import torch
+    import mphexplicit_b200 as M
+    from mphexplicit_b200 import scenes
+    sc = scenes.droplet_2d(n=40, seed=rank)
+    steps = args.droplet_steps
+    out = {"workload": "droplet_2d 40x40 fluid, no walls, surface tension: %d particles" % sc.n, "steps": steps,
+           "form": "fp64"}
+    res = {}
+    for graphs in (True, False):
+        s = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2, mode="fp64")
+        s.set_step_graphs(graphs)
+        s.step(3)  # warm-up (the first several-step call captures the graphs)
+        s.synchronize()
+        stream = torch.cuda.ExternalStream(s.stream_handle)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev0.record(stream)
+        s.step(steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3)
+        info = s.info()
+        st = s.state()
+        s.close()
+        res[graphs] = {"ms": ms, "st": st, "rebuilds": info["rebuild_count"]}
+        key = "graphs" if graphs else "host_path"
+        out[key] = {"value": sc.n * steps / (ms / 1e3), "ms_per_step": ms / steps, "rebuilds": info["rebuild_count"]}
+    out["bit_identical"] = all(np.array_equal(res[True]["st"][k], res[False]["st"][k]) for k in ("xyz", "vel"))
+    out["graphs_speedup_vs_host_path"] = res[False]["ms"] / res[True]["ms"]
+    out["value"] = out["graphs"]["value"]
+    from oracle import ref_inputs as RI
+    if rank == 0 and RI.ref_available(2) and not args.no_cpu_baseline:
+        cores = RI.host_cores()
+        with tempfile.TemporaryDirectory() as td:
+            d, g, n = RI.droplet_files(td, seed=rank)
+            ref = {}
+            for th in sorted({cores["logical"], 1}):
+                r = RI.time_reference(d, g, 2, 1, steps, th, timeout=1800)
+                ref[th] = {"value": n * r["steps"] / r["seconds"], "seconds": r["seconds"], "steps": r["steps"],
+                           "threads": th, "rebuilds": r["rebuilds"]}
+        best = max(ref.values(), key=lambda x: x["value"])
+        out["reference"] = {"kind": "reference (oracle/_ref/ref_mph2d, the reference's Mph_gcc2d flags)",
+                            "by_threads": list(ref.values()), "value": best["value"], "threads": best["threads"],
+                            "cores": cores}
+        out["graphs_vs_reference"] = out["graphs"]["value"] / best["value"]
+    return out
+
+
 def measure_two_fluid(args, rank):
     """Benchmark config 3: the two-fluid column (200^3 fluid, l0 = 0.0025 m,
     lower half type 0 at rho 500, upper half type 1 at rho 1000, interface
@@ -720,7 +776,8 @@ def main():
     ap.add_argument("--only", action="store_true", help="measure the headline form only")
     ap.add_argument("--scene", default="dam", choices=sorted(SCENES))
     ap.add_argument("--e2e-steps", type=int, default=10)
-    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,mixed_walk,learned,batch,two_fluid,output",
+    ap.add_argument("--droplet-steps", type=int, default=1000, help="steps of the 2-D droplet (config 1)")
+    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,mixed_walk,learned,batch,two_fluid,droplet,output",
                     help="forms to measure (comma list); the headline --mode must be among them for a full line")
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
@@ -785,6 +842,8 @@ def main():
         forms["batch"] = measure_batch(args, rank)
     if "two_fluid" in wanted:
         forms["two_fluid"] = measure_two_fluid(args, rank)
+    if "droplet" in wanted:
+        forms["droplet"] = measure_droplet(args, rank)
     if "output" in wanted:
         forms["output"] = measure_output(args, sc, rank)
     if args.mode not in res:  # a run of the extra forms alone (profiling)

@@ -64,6 +64,19 @@ struct LearnedState {
     mph_learned_info info{};
 };
 
+// mph_step in the FP64 form for more than one step: one executable graph per
+// parity of the velocity ping-pong, replayed once per step, whose conditional
+// nodes take the host's per-step decisions (the rebuild test and the table
+// check); made for the buffers and table capacities they were captured with.
+struct StepGraphs {
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // by the vcur of the step
+    int cur = -1, cap = -1, cap_s = -1;
+    const int* nlist = nullptr;
+    const int* nlist_s = nullptr;
+    int launches_step = 0, launches_rebuild = 0;  // kernels per step and per rebuild
+    bool enabled = true;
+};
+
 // mph_step_read_state: the copy stream (packs and device-to-host copies), its
 // events and the velocities' staging buffer; made by the first call.
 struct ReadBack {
@@ -96,6 +109,7 @@ struct mph_ctx {
     int max_neighbors = 0;
     long long launches = 0;
     ReadBack rb;
+    StepGraphs sg;
     Profiler prof;
     std::string err;
     mph::TextWriter* text = nullptr;  // *.prof / *.vtk writer thread, made by the first write
@@ -454,6 +468,8 @@ static int grow_list(mph_ctx* ctx, int need) { return grow_table(ctx, need, &ctx
 static bool uses_short_list(const mph_ctx* ctx) { return !ctx->sc.has_st; }
 
 // calculateCellParticle + calculateNeighbor (main.cpp:1111-1596).
+static int build_lists(mph_ctx* ctx);
+
 static int rebuild_fp64(mph_ctx* ctx) {
     mph::DevFP64& d = ctx->d;
     const SimConst& s = ctx->sc;
@@ -469,6 +485,16 @@ static int rebuild_fp64(mph_ctx* ctx) {
     }
     d.cur = b;
     d.vcur = vb;
+    return build_lists(ctx);
+}
+
+// calculateNeighbor on the current (just reordered) positions: the list and
+// the short sublist, growing their tables and building again while a list is
+// longer than its table.
+static int build_lists(mph_ctx* ctx) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
     const bool sl = uses_short_list(ctx);
     int max_short = 0;
     for (int attempt = 0; attempt < 3; ++attempt) {
@@ -577,6 +603,8 @@ extern "C" void mph_destroy(mph_ctx* ctx) {
         cudaFree(R.stage_v);
         if (R.copy) cudaStreamDestroy(R.copy);
     }
+    for (cudaGraphExec_t& e : ctx->sg.exec)
+        if (e) cudaGraphExecDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -697,7 +725,203 @@ static int step_fp64_head(mph_ctx* ctx) {
     return MPH_OK;
 }
 
+// ---- the FP64 step as CUDA graphs --------------------------------------------
+
+// Adds an IF node after the work captured so far on st and makes it the
+// capture's only dependency; *body is the graph the node runs.
+static int add_if_node(mph_ctx* ctx, cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    CUDA_TRY(ctx, cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    if (cs != cudaStreamCaptureStatusActive) return fail(ctx, MPH_ERR_CUDA, "step graph: no active capture");
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    CUDA_TRY(ctx, cudaGraphAddNode(&node, g, deps, nd, &p));
+    *body = p.conditional.phGraph_out[0];
+    CUDA_TRY(ctx, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return MPH_OK;
+}
+
+// Captures one FP64 step for vcur == v:
+//   gate -> IF run { memset, move, decide -> IF rebuild { cell index, bitonic
+//   sort, cell ranges, reorder (then copied back into the buffers this graph
+//   holds), pos32, neighbour list, table check }, IF sweep { sweep A, force
+//   sweep, step done } }
+// The same kernels with the same arguments as step_fp64, so the same bits.
+static int capture_step(mph_ctx* ctx, int v, cudaGraphExec_t* out, int* launches_step, int* launches_rebuild) {
+    mph::DevFP64& d = ctx->d;
+    const SimConst& s = ctx->sc;
+    cudaStream_t st = ctx->stream;
+    const int a = d.cur, b = 1 - d.cur, va = v, vb = 1 - v;
+    const size_t n = (size_t)ctx->n;
+    const bool sl = uses_short_list(ctx);
+    const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+    cudaGraph_t g = nullptr, g_run = nullptr, g_reb = nullptr, g_sw = nullptr;
+    cudaGraphConditionalHandle h_run = 0, h_reb = 0, h_sw = 0;
+    int rc = MPH_OK;
+    auto ck = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == MPH_OK)
+            rc = fail(ctx, MPH_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(e));
+        return rc == MPH_OK;
+    };
+    auto end_capture = [&]() {
+        cudaGraph_t tmp = nullptr;
+        ck(cudaStreamEndCapture(st, &tmp));
+        ck(cudaGetLastError());
+    };
+    int ls = 0, lr = 0;
+    if (ck(cudaGraphCreate(&g, 0)) && ck(cudaGraphConditionalHandleCreate(&h_run, g, 0, 0)) &&
+        ck(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode))) {
+        mph::launch_graph_gate(d.scal, h_run, st);
+        ++ls;
+        if (rc == MPH_OK) rc = add_if_node(ctx, st, h_run, &g_run);
+        end_capture();
+    }
+    if (rc == MPH_OK && ck(cudaGraphConditionalHandleCreate(&h_reb, g_run, 0, 0)) &&
+        ck(cudaGraphConditionalHandleCreate(&h_sw, g_run, 1, cudaGraphCondAssignDefault)) &&
+        ck(cudaStreamBeginCaptureToGraph(st, g_run, nullptr, nullptr, 0, mode))) {
+        ck(cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+        mph::launch_move(s, d.cellstart, d.pos[a], d.vel[va], d.snap, d.wall_center, d.scal, st);
+        mph::launch_graph_decide(d.scal, s.shift_thr, h_reb, st);
+        ls += 2;
+        if (rc == MPH_OK) rc = add_if_node(ctx, st, h_reb, &g_reb);
+        if (rc == MPH_OK) rc = add_if_node(ctx, st, h_sw, &g_sw);
+        end_capture();
+    }
+    if (rc == MPH_OK && ck(cudaStreamBeginCaptureToGraph(st, g_reb, nullptr, nullptr, 0, mode))) {
+        mph::launch_cell_index(s, d.pos[a], d.type[a], d.keys, d.vals, st);
+        lr += 1 + mph::launch_bitonic_sort(s, d.keys, d.vals, st);
+        mph::launch_cell_ranges(s, d.keys, d.cellstart, st);
+        mph::launch_reorder(s, d.vals, d.pidx[a], d.type[a], d.pos[a], d.vel[va], d.pidx[b], d.type[b], d.pos[b],
+                            d.vel[vb], d.snap, st);
+        ck(cudaMemcpyAsync(d.pos[a], d.pos[b], n * sizeof(double4), cudaMemcpyDeviceToDevice, st));
+        ck(cudaMemcpyAsync(d.vel[va], d.vel[vb], n * sizeof(double4), cudaMemcpyDeviceToDevice, st));
+        ck(cudaMemcpyAsync(d.pidx[a], d.pidx[b], n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        ck(cudaMemcpyAsync(d.type[a], d.type[b], n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        ck(cudaMemsetAsync(&d.scal->max_neighbors, 0, sizeof(int), st));
+        ck(cudaMemsetAsync(&d.scal->max_short, 0, sizeof(int), st));
+        mph::launch_pos32(s, d.pos[a], d.pos32, st);
+        mph::launch_neighbor_list(s, d.pos[a], d.pos32, d.cellstart, d.ncount, d.nlist, d.cap,
+                                  sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.cap_s, d.scal, st);
+        mph::launch_graph_list_check(d.scal, d.cap, d.cap_s, sl ? 1 : 0, h_sw, st);
+        lr += 6;
+        end_capture();
+    }
+    if (rc == MPH_OK && ck(cudaStreamBeginCaptureToGraph(st, g_sw, nullptr, nullptr, 0, mode))) {
+        mph::launch_sweep_a(s, d.cellstart, d.pos[a], d.vel[va], d.ncount, d.nlist, d.ncount_s, d.nlist_s,
+                            d.dens_a, d.strain_p, d.div_p, d.press, d.gc, d.wall_center, st);
+        mph::launch_sweep_b(s, d.cellstart, d.pos[a], d.vel[va], d.vel[vb], d.press, d.gc, d.ncount, d.nlist,
+                            sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force, d.scal, st, nullptr,
+                            nullptr, nullptr, 1);
+        mph::launch_graph_step_done(d.scal, st);
+        ls += 3;
+        end_capture();
+    }
+    if (rc == MPH_OK) ck(cudaGraphInstantiate(out, g, 0));
+    if (g) cudaGraphDestroy(g);
+    *launches_step = ls;
+    *launches_rebuild = lr;
+    return rc;
+}
+
+static void drop_step_graphs(mph_ctx* ctx) {
+    StepGraphs& G = ctx->sg;
+    for (cudaGraphExec_t& e : G.exec)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+    G.cur = -1;
+}
+
+static int ensure_step_graphs(mph_ctx* ctx) {
+    StepGraphs& G = ctx->sg;
+    const mph::DevFP64& d = ctx->d;
+    if (G.exec[0] && G.exec[1] && G.cur == d.cur && G.cap == d.cap && G.cap_s == d.cap_s && G.nlist == d.nlist &&
+        G.nlist_s == d.nlist_s)
+        return MPH_OK;
+    drop_step_graphs(ctx);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int v = 0; v < 2; ++v) {
+        const int rc = capture_step(ctx, v, &G.exec[v], &G.launches_step, &G.launches_rebuild);
+        if (rc != MPH_OK) {
+            drop_step_graphs(ctx);
+            return rc;
+        }
+    }
+    G.cur = d.cur;
+    G.cap = d.cap;
+    G.cap_s = d.cap_s;
+    G.nlist = d.nlist;
+    G.nlist_s = d.nlist_s;
+    return MPH_OK;
+}
+
+// nsteps FP64 steps as graph launches with no host round trip in between;
+// the host reads the batch's counters at the end.  A list that outgrew its
+// table stops the batch after that step's reorder: the host then grows the
+// table, builds the list again from the same positions, finishes that step
+// and runs the rest.  A non-finite velocity is reported at the end of the
+// batch (the host path reports it at the next step's move).
+static int step_fp64(mph_ctx* ctx, int nsteps);
+
+static int step_fp64_graphs(mph_ctx* ctx, int nsteps) {
+    StepGraphs& G = ctx->sg;
+    mph::DevFP64& d = ctx->d;
+    cudaStream_t st = ctx->stream;
+    TRY(ensure_step_graphs(ctx));
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->stop, 0, 3 * sizeof(int), st));  // stop, steps_done, rebuilds_done
+    for (int k = 0; k < nsteps; ++k) CUDA_TRY(ctx, cudaGraphLaunch(G.exec[(d.vcur + k) & 1], st));
+    TRY(read_scalars(ctx));
+    const StepScalars& h = *ctx->h_scal;
+    const int done = h.steps_done, reb = h.rebuilds_done, stopped = h.stop;
+    for (int k = 0; k < done; ++k) ctx->time += ctx->p.dt;  // main.cpp:449, one step at a time
+    ctx->step += done;
+    if (done & 1) d.vcur = 1 - d.vcur;
+    ctx->rebuilds += reb;
+    ctx->launches += (long long)G.launches_step * (done + stopped) + (long long)G.launches_rebuild * reb;
+    if (reb > 0) {
+        ctx->max_neighbors = h.max_neighbors;
+        ctx->lrn.edges_valid = false;
+    }
+    ctx->dens_a_valid = ctx->sc.has_st;
+    ctx->lazy_pos = -1;
+    ctx->wall_force_valid = false;
+    ctx->virial_valid = false;
+    if (h.flags & ~mph::DEVFLAG_NEIGHBOR_OVERFLOW) return check_flags(ctx);
+    if (!stopped) {
+        if (done != nsteps) return fail(ctx, MPH_ERR_DEVICE, "step graph: a step did not complete");
+        return MPH_OK;
+    }
+    // the stopped step: moved, sorted and reordered; build its lists with room
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->flags, 0, sizeof(int), st));
+    TRY(build_lists(ctx));
+    sweep_a(ctx, true);
+    {
+        Launch L(ctx, "sweep_b");
+        const bool sl = uses_short_list(ctx);
+        mph::launch_sweep_b(ctx->sc, d.cellstart, d.pos[d.cur], d.vel[d.vcur], d.vel[1 - d.vcur], d.press, d.gc,
+                            d.ncount, d.nlist, sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force, d.scal,
+                            st, nullptr, nullptr, nullptr, 1);
+        ctx->wall_force_valid = false;
+    }
+    d.vcur = 1 - d.vcur;
+    CUDA_TRY(ctx, cudaGetLastError());
+    ctx->time += ctx->p.dt;
+    ++ctx->step;
+    const int rest = nsteps - done - 1;
+    return rest > 0 ? step_fp64(ctx, rest) : MPH_OK;
+}
+
 static int step_fp64(mph_ctx* ctx, int nsteps) {
+    // several steps: graph replay (per-kernel profiling needs the host path)
+    if (nsteps > 1 && ctx->sg.enabled && !ctx->prof.on) return step_fp64_graphs(ctx, nsteps);
     mph::DevFP64& d = ctx->d;
     const SimConst& s = ctx->sc;
     cudaStream_t st = ctx->stream;
@@ -974,6 +1198,13 @@ extern "C" int mph_step(mph_ctx* ctx, int nsteps) {
     if (ctx->mixed) return step_mixed(ctx, nsteps);
     if (ctx->mode == MPH_MODE_LEARNED) return step_learned(ctx, nsteps);
     return step_fp64(ctx, nsteps);
+}
+
+extern "C" int mph_set_step_graphs(mph_ctx* ctx, int enable) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    ctx->sg.enabled = enable != 0;
+    if (!enable) drop_step_graphs(ctx);
+    return MPH_OK;
 }
 
 extern "C" int mph_synchronize(mph_ctx* ctx) {

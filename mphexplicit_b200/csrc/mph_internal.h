@@ -60,7 +60,10 @@ struct StepScalars {
     int max_neighbors;                   // longest list of the last build
     int rebuild;                         // decision of the last move kernel
     int max_short, max_long;             // longest short / long part (mixed table)
-    int pad[9];
+    int stop;                            // step graphs: a list overflowed, the later steps skip
+    int steps_done;                      // step graphs: steps completed in this batch
+    int rebuilds_done;                   // step graphs: rebuilds started in this batch
+    int pad[6];
 };
 
 enum : int {
@@ -130,6 +133,17 @@ void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* p
                           int* ncount, int* nlist, int cap, int* ncount_s, int* nlist_s, int cap_s,
                           StepScalars* scal, cudaStream_t s);
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);
+
+// ---- step graphs (FP64 form; the control kernels of k_cells.cu) ----------
+// gate: run = 1 unless an earlier step of the batch stopped
+void launch_graph_gate(StepScalars* scal, cudaGraphConditionalHandle run, cudaStream_t s);
+// rebuild test of main.cpp:1102 on the move kernel's maximum shift
+void launch_graph_decide(StepScalars* scal, double shift_thr, cudaGraphConditionalHandle rebuild,
+                         cudaStream_t s);
+// after a list build: a list longer than its table stops the batch (sweep = 0)
+void launch_graph_list_check(StepScalars* scal, int cap, int cap_s, int short_list,
+                             cudaGraphConditionalHandle sweep, cudaStream_t s);
+void launch_graph_step_done(StepScalars* scal, cudaStream_t s);
 void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s);
 
 // ---- kernel launchers (k_fp64.cu) -----------------------------------------

@@ -312,6 +312,10 @@ class Solver:
         _check(self._lib.mph_get_state(self._ctx, None, None, _dp(xyz), _dp(vel), None, None, None, None, None),
                self._ctx)
 
+    def set_step_graphs(self, enable: bool) -> None:
+        """Graph launches for several FP64 steps (default) or the host path."""
+        _check(self._lib.mph_set_step_graphs(self._ctx, 1 if enable else 0), self._ctx)
+
     def step_read_state(self, nsteps: int, xyz: np.ndarray | None, vel: np.ndarray | None) -> None:
         """step(nsteps), then the positions and velocities after it into caller
         arrays (sorted order, C-contiguous float64 [n, 3]); the FP64 form copies

@@ -7,7 +7,8 @@ the reference runs the reference's code and nothing of the product.
 
 * ``dam_break_arrays``: the seeded 3-D dam-break scene (fluid block of type 0 in
   the corner of a box closed by type-2 wall layers), the same arrays as the
-  product's scene generator (a CPU test compares them element for element).
+  product's scene generator (a CPU test compares them element for element);
+  ``droplet_arrays``: the 2-D square droplet, likewise.
 * ``write_data`` / ``write_grid``: the reference's *.data keys (readDataFile,
   source/main.cpp:502-521) and *.grid layout (readGridFile, main.cpp:541-640;
   the generator's writer, generator/generator.cpp:197-217).
@@ -80,6 +81,30 @@ def dam_break_arrays(fluid=(100, 100, 200), box=(300, 100, 240), l0=0.005, walls
               "wall_velocity": [[0.0] * 3 for _ in range(4)], "wall_omega": [[0.0] * 3 for _ in range(4)]}
     header = {"time": 0.0, "n": len(xyz), "l0": l0, "dmin": dmin, "dmax": dmax}
     return params, header, typ, xyz, np.zeros_like(xyz)
+
+
+def droplet_arrays(n=40, l0=0.004, seed=0, box=100.0, steps=1000, rho=1000.0, mu=0.1, sigma=0.07, c_sound=10.0,
+                   dt=1.0e-5):
+    """(params dict, header dict, type, xyz, vel) of the 2-D square droplet:
+    n x n type-0 particles on a lattice with a seeded uniform +-0.01 l0 jitter,
+    no walls, no gravity, surface tension sigma; the domain `box` cells wide,
+    padded so no pair interacts across the periodic boundary."""
+    rng = np.random.default_rng(seed)
+    xy = _lattice((n, n), l0, (-0.5 * n * l0, -0.5 * n * l0))
+    xy += rng.uniform(-0.01 * l0, 0.01 * l0, xy.shape)
+    xyz = np.zeros((len(xy), 3))
+    xyz[:, :2] = xy
+    half = 0.5 * (box + 2 * _pad_for_cells(box, 0.0) - box) + 0.5 * box
+    four = lambda v: [float(v)] * 4  # noqa: E731
+    params = {"dt": dt, "output_interval": 1.0e30, "vtk_output_interval": 1.0e30, "end_time": dt * (steps - 0.5),
+              "radius_ratio_a": 3.5, "radius_ratio_p": 1.7, "radius_ratio_v": 3.5, "density": four(rho),
+              "bulk_modulus": four(rho * c_sound ** 2), "bulk_viscosity": four(mu), "shear_viscosity": four(mu),
+              "surface_tension": four(sigma), "interaction_ratio": [[1.0] * 4 for _ in range(4)],
+              "gravity": [0.0, 0.0, 0.0], "wall_center": [[0.0] * 3 for _ in range(4)],
+              "wall_velocity": [[0.0] * 3 for _ in range(4)], "wall_omega": [[0.0] * 3 for _ in range(4)]}
+    header = {"time": 0.0, "n": len(xyz), "l0": l0, "dmin": [-half * l0, -half * l0, -0.5 * l0],
+              "dmax": [half * l0, half * l0, 0.5 * l0]}
+    return params, header, np.zeros(len(xyz), np.int32), xyz, np.zeros_like(xyz)
 
 
 def write_data(path: str, p: dict) -> None:
@@ -177,3 +202,13 @@ def dam_break_files(td: str, seed: int = 0, **kw):
     write_data(d, p)
     write_grid(g, h, t, x, v)
     return d, g, int(h["n"]), int(np.count_nonzero(t < 2))
+
+
+def droplet_files(td: str, seed: int = 0, **kw):
+    """Write the 2-D droplet's *.data / *.grid into directory td; returns
+    (data path, grid path, particles)."""
+    p, h, t, x, v = droplet_arrays(seed=seed, **kw)
+    d, g = os.path.join(td, "drop.data"), os.path.join(td, "drop.grid")
+    write_data(d, p)
+    write_grid(g, h, t, x, v)
+    return d, g, int(h["n"])

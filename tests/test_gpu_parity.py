@@ -291,6 +291,66 @@ def test_neighbor_table_grows_on_compression():
     assert_same(i1, i2, "nind")
 
 
+INFO_KEYS = ("step", "rebuild_count", "time", "max_neighbor_count", "neighbor_capacity")
+
+
+@pytest.mark.parametrize("name", ["dam_break_small", "two_fluid_small", "moving_walls", "droplet_2d", "bridge"])
+def test_step_graphs_match_host_path(name):
+    """Several FP64 steps per mph_step run as graph launches whose conditional
+    nodes take the rebuild test on the device; the host path (one flag read
+    per step) gives the same bits, rebuilds, step count and time."""
+    case = GoldenCase(name)
+    a, b = solver_for(case), solver_for(case)
+    b.set_step_graphs(False)
+    done = 0
+    for m in (1, 2, 7, 13, case.steps):
+        m = min(m, case.steps - done)
+        if m <= 0:
+            break
+        a.step(m)
+        b.step(m)
+        done += m
+    a.synchronize()
+    b.synchronize()
+    ia, ib = a.info(), b.info()
+    for k in INFO_KEYS:
+        assert ia[k] == ib[k], (k, ia[k], ib[k])
+    if name in ("dam_break_small", "moving_walls"):
+        assert ia["rebuild_count"] > 0
+    sa, sb = a.state(), b.state()
+    for key in STATE_KEYS:
+        if key != "virial_pressure":
+            assert_same(sa[key], sb[key], key)
+    fa, fb = a.fields(), b.fields()
+    for key in FIELD_KEYS:
+        assert_same(fa[key], fb[key], key)
+
+
+def test_step_graphs_grow_the_table_mid_batch():
+    """A list that outgrows its table inside a batch of graph launches stops
+    the batch after that step's reorder; the host grows the table, builds the
+    list again and finishes the steps: the same bits as the host path."""
+    sc = scenes.droplet_2d(n=20, seed=9)
+    a = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
+    b = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
+    b.set_step_graphs(False)
+    cap0 = a.info()["neighbor_capacity"]
+    for s in (a, b):
+        st = s.state()
+        c = st["xyz"].mean(axis=0)
+        s.set_state(c + (st["xyz"] - c) * 0.6, st["vel"])
+        s.step(6)
+        s.synchronize()
+    ia, ib = a.info(), b.info()
+    assert ia["neighbor_capacity"] > cap0
+    for k in INFO_KEYS:
+        assert ia[k] == ib[k], (k, ia[k], ib[k])
+    sa, sb = a.state(), b.state()
+    for key in STATE_KEYS:
+        if key != "virial_pressure":
+            assert_same(sa[key], sb[key], key)
+
+
 def test_full_size_dam_break_two_steps():
     """Benchmark config 2 at full size (2.0 M fluid + 0.78 M wall): two steps,
     bit-exact against the oracle, and the expected interior neighbour count."""

@@ -39,6 +39,21 @@ def test_dam_break_arrays_equal_product_scene(fluid, box, seed):
         assert open(g1, "rb").read() == open(g2, "rb").read()
 
 
+@pytest.mark.parametrize("n,seed", [(40, 0), (12, 5)])
+def test_droplet_arrays_equal_product_scene(n, seed):
+    sc = scenes.droplet_2d(n=n, seed=seed)
+    p, h, t, x, v = RI.droplet_arrays(n=n, seed=seed)
+    assert np.array_equal(t, sc.type) and np.array_equal(x, sc.xyz) and np.array_equal(v, sc.vel)
+    with tempfile.TemporaryDirectory() as td:
+        d1, g1 = os.path.join(td, "a.data"), os.path.join(td, "a.grid")
+        d2, g2 = os.path.join(td, "b.data"), os.path.join(td, "b.grid")
+        sc.write(d1, g1)
+        RI.write_data(d2, p)
+        RI.write_grid(g2, h, t, x, v)
+        assert open(d1, "rb").read() == open(d2, "rb").read()
+        assert open(g1, "rb").read() == open(g2, "rb").read()
+
+
 def test_host_cores():
     c = RI.host_cores()
     assert c["logical"] >= 1 and 1 <= c["physical"] <= c["logical"]
