@@ -230,18 +230,19 @@ int mph_create(const mph_params* p, const mph_grid_header* h, int dim, int mode,
 
 /* Advance nsteps explicit steps: the loop body main.cpp:386-431 plus
  * Time += Dt (main.cpp:449).  No file output.  Returns when the steps are
- * done.  One step (and every step of the mixed and learned forms): the
- * host reads the neighbour-rebuild test's flag after the move.  Several FP64
- * steps: one CUDA graph launch per step, whose conditional nodes make that
- * test (and check the rebuilt list against its table) on the device, with no
- * host round trip until the end; the same kernels, so the same bits.  A list
- * that outgrows its table ends the graph launches after that step's reorder;
- * the host grows the table and finishes the steps.  With profiling on
- * (mph_profile_enable) the host path runs. */
+ * done.  Each step the host reads the neighbour-rebuild test's flag after the
+ * move (see mph_set_step_graphs for the alternative). */
 int mph_step(mph_ctx* ctx, int nsteps);
 
-/* enable == 0: mph_step takes the host path for every step (for comparison
- * and debugging); 1 (the default): graph launches for several FP64 steps. */
+/* enable == 1: mph_step of several FP64 steps runs one CUDA graph launch per
+ * step, whose conditional nodes make the rebuild test (and check the rebuilt
+ * list against its table) on the device, with no host round trip until the
+ * end; the same kernels, so the same bits.  A list that outgrows its table
+ * ends the graph launches after that step's reorder; the host grows the table
+ * and finishes the steps.  With profiling on (mph_profile_enable) the host
+ * path runs.  0 (the default): the host path.  Measured on one B200, scenes
+ * of 1.6 k to 2.8 M particles: within +-3 % of the host path either way (the
+ * per-step read costs about what the graph's control kernels do). */
 int mph_set_step_graphs(mph_ctx* ctx, int enable);
 
 /* Wait for the context's stream and report any device-side error flag. */

@@ -520,6 +520,322 @@ k_sweep_b(SimConst c, const int* __restrict__ cellstart, const double4* __restri
     }
 }
 
+// ---- warp per particle (small scenes) ----------------------------------------
+// With few particles the thread-per-particle sweeps leave most of the GPU idle
+// and each thread's chain of dependent FP64 work over its ~200 list entries
+// sets the time.  Here a warp takes one particle: its 32 lanes compute the
+// pair terms of 32 consecutive list entries at once (the expressions of
+// k_sweep_a / k_sweep_b), then one lane per sum adds the chunk's terms to it
+// in list order, each with the operation the thread kernels apply (+= or -=,
+// two in a row where they apply two): the same additions in the same order,
+// so the same bits.
+constexpr int kWarpSweepWarps = 4;
+
+// lane s's sum of k_sweep_b_w: flag bit, first term, second term (-1: none), subtract
+struct SumOp {
+    unsigned bit;
+    int q1, q2;
+    bool sub;
+};
+__device__ __forceinline__ SumOp sweep_b_sum(int s) {
+    // fp0..2 (+, bit 1), fv0..2 (+, bit 8), fa0..2 (+, bit 2), fd0..2 (-, -, bit 4)
+    if (s < 3) return {1u, s, -1, false};
+    if (s < 6) return {8u, s, -1, false};
+    if (s < 9) return {2u, s, -1, false};
+    return {4u, s, s + 3, true};
+}
+
+template <bool ST, bool RATIO>
+__global__ void __launch_bounds__(32 * kWarpSweepWarps)
+k_sweep_b_w(SimConst c, const int* __restrict__ cellstart, const double4* __restrict__ pos,
+            const double4* __restrict__ velp, double4* __restrict__ vel_out, const double4* __restrict__ gcpa,
+            const int* __restrict__ ncount, const int* __restrict__ nlist, double4* __restrict__ force,
+            StepScalars* __restrict__ scal, int part, double* __restrict__ vel_host) {
+    constexpr int NV = ST ? 15 : 6;  // terms per entry: fp 3, fv 3 [, fa 3, fd 3 + 3]
+    constexpr int NS = ST ? 12 : 6;  // sums
+    __shared__ double tv[kWarpSweepWarps][NV][33];
+    __shared__ unsigned tf[kWarpSweepWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * kWarpSweepWarps + w;
+    if (i >= c.n) return;  // whole warp
+    const int nf = cellstart[c.tot];
+    const double4 vi = velp[i];   // .w = PressureP
+    if (part == 1 && i >= nf) {   // a wall keeps its velocity (see k_sweep_b)
+        if (lane == 0) {
+            vel_out[i] = make_double4(vi.x, vi.y, vi.z, 0.0);
+            if (vel_host) {
+                vel_host[3 * (size_t)i] = vi.x;
+                vel_host[3 * (size_t)i + 1] = vi.y;
+                vel_host[3 * (size_t)i + 2] = vi.z;
+            }
+        }
+        return;
+    }
+    if (part == 2 && i < nf) return;
+    const double4 pi = pos[i];
+    const int ti = type_of(pi);
+    const double ai = c.a_k[ti];
+    double4 gci = make_double4(0, 0, 0, 0);
+    if (ST) gci = gcpa[i];        // .w = PressureA
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    const SumOp op = sweep_b_sum(lane < NS ? lane : 0);
+    double acc = 0.0;
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int k = k0 + lane;
+        unsigned fl = 0u;
+        double v[NV];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q] = 0.0;
+        const int j = k < cnt ? __ldg(nlist + (size_t)k * n + i) : i;
+        if (j != i) {
+            const double4 pj = pos[j];
+            double x[3];
+            disp(c, pi, pj, x);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            const bool in_p = r2 < c.rp2;
+            const bool in_a = ST && (r2 < c.ra2);
+            const bool in_g = ST && (r2 < c.rg2);
+            const bool in_v = r2 < c.rv2;
+            if (in_p || in_a || in_g || in_v) {
+                const double4 vj = velp[j];   // .w = PressureP of j
+                const int tj = type_of(pj);
+                const double r = sqrt(r2);
+                const double ri = __drcp_rn(r);
+                const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
+                const double qa = div_rs(r, c.ra, c.inv_ra);
+                double rij = 1.0, rji = 1.0;
+                if (RATIO) { rij = c.ratio[ti][tj]; rji = c.ratio[tj][ti]; }
+                if (in_p) {
+                    const double qp = div_rs(r, c.rp, c.inv_rp);
+                    const double dw = s_dwp(c, qp);
+                    const double gw0 = div_rs(dw * x[0], r, ri), gw1 = div_rs(dw * x[1], r, ri),
+                                 gw2 = div_rs(dw * x[2], r, ri);
+                    const double ps = vi.w + vj.w;
+                    v[0] = ps * gw0 * c.vol;
+                    v[1] = ps * gw1 * c.vol;
+                    v[2] = ps * gw2 * c.vol;
+                    fl |= 1u;
+                }
+                if (in_v) {
+                    const double qv = c.rv_eq_ra ? qa : div_rs(r, c.rv, c.inv_rv);
+                    const double dw = -s_dwv(c, qv);
+                    const double u0 = vj.x - vi.x, u1 = vj.y - vi.y, u2 = vj.z - vi.z;
+                    const double cm = c.visc_mu[ti][tj];
+                    const double dot = u0 * e0 + u1 * e1 + u2 * e2;
+                    v[3] = div_rs(cm * dot * e0 * dw, r, ri) * c.vol;
+                    v[4] = div_rs(cm * dot * e1 * dw, r, ri) * c.vol;
+                    v[5] = div_rs(cm * dot * e2 * dw, r, ri) * c.vol;
+                    fl |= 8u;
+                }
+                if (ST && in_a) {
+                    const double dwa = s_dwa(c, qa);
+                    const double dwij = RATIO ? rij * dwa : dwa;
+                    const double dwji = RATIO ? rji * dwa : dwa;
+                    const double sa = gci.w * dwij + gcpa[j].w * dwji;
+                    v[6 % NV] = sa * e0 * c.vol;
+                    v[7 % NV] = sa * e1 * c.vol;
+                    v[8 % NV] = sa * e2 * c.vol;
+                    fl |= 2u;
+                }
+                if (ST && in_g) {
+                    const double4 gcj = gcpa[j];
+                    const double aj = ai;
+                    const double qg = c.rg_eq_ra ? qa : div_rs(r, c.rg, c.inv_rg);
+                    const double wg = s_wg(c, qg);
+                    const double wij = RATIO ? rij * wg : wg;
+                    const double wji = RATIO ? rji * wg : wg;
+                    v[9 % NV] = div_rs(aj * gcj.x * wji - ai * gci.x * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    v[10 % NV] = div_rs(aj * gcj.y * wji - ai * gci.y * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    v[11 % NV] = div_rs(aj * gcj.z * wji - ai * gci.z * wij, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    const double dg = s_dwg(c, qg);
+                    const double dwij = RATIO ? rij * dg : dg;
+                    const double dwji = RATIO ? rji * dg : dg;
+                    double gr = 0.0;
+                    gr += (aj * gcj.x * dwji - ai * gci.x * dwij) * x[0];
+                    gr += (aj * gcj.y * dwji - ai * gci.y * dwij) * x[1];
+                    gr += (aj * gcj.z * dwji - ai * gci.z * dwij) * x[2];
+                    v[12 % NV] = div_rs((gr) * e0, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    v[13 % NV] = div_rs((gr) * e1, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    v[14 % NV] = div_rs((gr) * e2, c.r2g, c.inv_r2g) * c.rg * c.vol_over_l0;
+                    fl |= 4u;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NV; ++q) tv[w][q][lane] = v[q];
+        tf[w][lane] = fl;
+        __syncwarp();
+        const int m = min(32, cnt - k0);
+        if (lane < NS) {
+            for (int e = 0; e < m; ++e) {
+                if (tf[w][e] & op.bit) {
+                    if (op.sub) {
+                        acc -= tv[w][op.q1][e];
+                        acc -= tv[w][op.q2][e];
+                    } else {
+                        acc += tv[w][op.q1][e];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    double sums[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) sums[q] = q < NS ? __shfl_sync(0xffffffffu, acc, q) : 0.0;
+    if (lane != 0) return;
+    const double fp0 = sums[0], fp1 = sums[1], fp2 = sums[2];
+    const double fv0 = sums[3], fv1 = sums[4], fv2 = sums[5];
+    const double fa0 = sums[6], fa1 = sums[7], fa2 = sums[8];
+    const double fd0 = sums[9], fd1 = sums[10], fd2 = sums[11];
+    double F0 = 0.0, F1 = 0.0, F2 = 0.0;   // resetForce (main.cpp:1617-1628), as k_sweep_b
+    F0 += fp0; F1 += fp1; F2 += fp2;
+    F0 += fa0; F1 += fa1; F2 += fa2;
+    F0 += fd0; F1 += fd1; F2 += fd2;
+    F0 += fv0; F1 += fv1; F2 += fv2;
+    double4 vn = make_double4(vi.x, vi.y, vi.z, 0.0);
+    if (i < nf) {
+        const double m = c.density[ti] * c.vol;
+        F0 += m * c.gravity[0];
+        F1 += m * c.gravity[1];
+        F2 += m * c.gravity[2];
+        vn.x += F0 / m * c.dt;
+        vn.y += F1 / m * c.dt;
+        vn.z += F2 / m * c.dt;
+        if (!(isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z))) atomicOr(&scal->flags, DEVFLAG_NONFINITE);
+    }
+    force[i] = make_double4(F0, F1, F2, 0.0);
+    if (part != 2) {
+        vel_out[i] = vn;
+        if (vel_host) {
+            vel_host[3 * (size_t)i] = vn.x;
+            vel_host[3 * (size_t)i + 1] = vn.y;
+            vel_host[3 * (size_t)i + 2] = vn.z;
+        }
+    }
+}
+
+// Sweep A, warp per particle: sums DensityA (lane 0, bit 1), DensityP (lane 1,
+// bit 2), DivergenceP (lane 2, bit 2, three subtractions per entry) and
+// GravityCenter (lanes 3-5, bit 4), as k_sweep_a adds them.
+template <bool ST, bool RATIO, bool DA>
+__global__ void __launch_bounds__(32 * kWarpSweepWarps)
+k_sweep_a_w(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
+            const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
+            double* __restrict__ strain_p, double* __restrict__ div_p, double4* __restrict__ velp,
+            double4* __restrict__ gcpa, double* __restrict__ wall_center) {
+    __shared__ double tv[kWarpSweepWarps][8][33];
+    __shared__ unsigned tf[kWarpSweepWarps][32];
+    if (wall_center != nullptr && blockIdx.x == 0 && threadIdx.x < 12) {
+        // WallCenter += WallVelocity*Dt (main.cpp:2048-2052), as k_sweep_a
+        const int t = threadIdx.x / 3, d = threadIdx.x % 3;
+        if (t >= 2) wall_center[3 * t + d] += c.wall_velocity[t][d] * c.dt;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * kWarpSweepWarps + w;
+    if (i >= c.n) return;  // whole warp
+    const double4 pi = pos[i];
+    const double4 vi = vel[i];
+    const int ti = type_of(pi);
+    const int cnt = ncount[i];
+    const size_t n = (size_t)c.n;
+    // lane s's sum: 0 DensityA, 1 DensityP, 2 DivergenceP, 3-5 GravityCenter
+    const unsigned bit = lane == 0 ? 1u : (lane < 3 ? 2u : 4u);
+    double acc = 0.0;
+    for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int k = k0 + lane;
+        unsigned fl = 0u;
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = 0.0;
+        const int j = k < cnt ? __ldg(nlist + (size_t)k * n + i) : i;
+        if (j != i) {
+            const double4 pj = pos[j];
+            double x[3];
+            disp(c, pi, pj, x);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            const bool in_a = DA && (r2 <= c.ra2);
+            const bool in_p = r2 <= c.rp2;
+            const bool in_g = ST && (r2 <= c.rg2);
+            if (in_a || in_p || in_g) {
+                const double r = sqrt(r2);
+                double ratio = 1.0;
+                if (RATIO) ratio = c.ratio[ti][type_of(pj)];
+                const double qa = div_rs(r, c.ra, c.inv_ra);
+                if (in_a) {
+                    v[0] = RATIO ? ratio * s_wa(c, qa) : s_wa(c, qa);
+                    fl |= 1u;
+                }
+                if (ST && in_g) {
+                    const double qg = c.rg_eq_ra ? qa : div_rs(r, c.rg, c.inv_rg);
+                    const double wgt = RATIO ? ratio * s_wg(c, qg) : s_wg(c, qg);
+                    v[5] = div_rs(x[0] * wgt, c.r2g, c.inv_r2g) * c.rg;
+                    v[6] = div_rs(x[1] * wgt, c.r2g, c.inv_r2g) * c.rg;
+                    v[7] = div_rs(x[2] * wgt, c.r2g, c.inv_r2g) * c.rg;
+                    fl |= 4u;
+                }
+                if (in_p) {
+                    const double4 vjn = vel[j];
+                    const double qp = div_rs(r, c.rp, c.inv_rp);
+                    v[1] = s_wp(c, qp);
+                    const double dw = s_dwp(c, qp);
+                    const double ri = __drcp_rn(r);
+                    const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
+                    const double u0 = vjn.x - vi.x, u1 = vjn.y - vi.y, u2 = vjn.z - vi.z;
+                    v[2] = u0 * e0 * dw;
+                    v[3] = u1 * e1 * dw;
+                    v[4] = u2 * e2 * dw;
+                    fl |= 2u;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) tv[w][q][lane] = v[q];
+        tf[w][lane] = fl;
+        __syncwarp();
+        const int m = min(32, cnt - k0);
+        if (lane < 6) {
+            for (int e = 0; e < m; ++e) {
+                if (tf[w][e] & bit) {
+                    if (lane == 0) acc += tv[w][0][e];
+                    else if (lane == 1) acc += tv[w][1][e];
+                    else if (lane == 2) {
+                        acc -= tv[w][2][e];
+                        acc -= tv[w][3][e];
+                        acc -= tv[w][4][e];
+                    } else {
+                        acc += tv[w][lane + 2][e];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    const double sum_a = __shfl_sync(0xffffffffu, acc, 0);
+    const double sum_p = __shfl_sync(0xffffffffu, acc, 1);
+    const double sum_d = __shfl_sync(0xffffffffu, acc, 2);
+    const double g0 = __shfl_sync(0xffffffffu, acc, 3);
+    const double g1 = __shfl_sync(0xffffffffu, acc, 4);
+    const double g2 = __shfl_sync(0xffffffffu, acc, 5);
+    if (lane != 0) return;
+    if (DA) dens_a[i] = sum_a;
+    const double strain = sum_p - c.n0p;
+    strain_p[i] = strain;
+    div_p[i] = sum_d;
+    double kappa = c.bulk_modulus[ti];
+    if (strain < 0.0) kappa = 0.0;
+    const double lambda = c.bulk_viscosity[ti];
+    const double pp = -lambda * sum_d + kappa * strain;
+    double pa = 0.0;
+    if (DA) {
+        pa = c.cof_a[ti] * (sum_a - c.n0a) / c.l0;
+        if (c.n0a <= sum_a) pa = 0.0;
+    }
+    velp[i] = make_double4(vi.x, vi.y, vi.z, pp);
+    gcpa[i] = make_double4(ST ? g0 : 0.0, ST ? g1 : 0.0, ST ? g2 : 0.0, pa);
+}
+
 // Self-check of div_rn against the hardware IEEE division: operands with
 // random significands and exponents in [-40, 40], plus all-ones significands.
 __global__ void k_check_division(unsigned long long seed, long long n, unsigned long long* mismatches,
@@ -660,6 +976,13 @@ k_conserved(SimConst c, const int* __restrict__ cellstart, const double4* __rest
 }
 
 inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+// Small scenes take the warp-per-particle sweeps: below this many particles
+// the thread-per-particle sweeps leave most of the GPU idle.
+#ifndef MPH_WARP_SWEEP_MAX_N
+#define MPH_WARP_SWEEP_MAX_N 65536
+#endif
+inline bool use_warp_sweeps(const SimConst& c) { return c.n <= MPH_WARP_SWEEP_MAX_N; }
 
 // ---- learned form ----------------------------------------------------------
 
@@ -865,10 +1188,15 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
                     double* strain_p, double* div_p, double4* press, double4* gc, double* wall_center,
                     cudaStream_t s) {
     (void)cellstart;
-    const int nb = blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1;
+    const bool warp = use_warp_sweeps(c);
+    const int nb = warp ? blocks(c.n, kWarpSweepWarps) : (blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1);
 #define SWEEP_A(ST, RATIO, CNT, LIST)                                                                             \
-    k_sweep_a<ST, RATIO, ST><<<nb, 128, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p, div_p, press, gc, \
-                                                wall_center)
+    if (warp)                                                                                                     \
+        k_sweep_a_w<ST, RATIO, ST><<<nb, 32 * kWarpSweepWarps, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p,  \
+                                                                       div_p, press, gc, wall_center);            \
+    else                                                                                                          \
+        k_sweep_a<ST, RATIO, ST><<<nb, 128, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p, div_p, press, gc,   \
+                                                    wall_center)
     if (c.has_st) {
         if (c.ratio_all_one) SWEEP_A(true, false, ncount, nlist); else SWEEP_A(true, true, ncount, nlist);
     } else {
@@ -894,6 +1222,19 @@ void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
     (void)vel_in;
     if (i1 < 0) i1 = c.n;
     if (i1 <= i0) return;
+    if (!eforce && i0 == 0 && i1 == c.n && use_warp_sweeps(c)) {
+        const int nw = blocks(c.n, kWarpSweepWarps);
+#define SWEEP_BW(ST, RATIO)                                                                                       \
+    k_sweep_b_w<ST, RATIO><<<nw, 32 * kWarpSweepWarps, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount,    \
+                                                              nlist, force, scal, part, vel_host)
+        if (c.has_st) {
+            if (c.ratio_all_one) SWEEP_BW(true, false); else SWEEP_BW(true, true);
+        } else {
+            if (c.ratio_all_one) SWEEP_BW(false, false); else SWEEP_BW(false, true);
+        }
+#undef SWEEP_BW
+        return;
+    }
     const int nb = blocks(i1 - i0, 128);
 #define SWEEP_B(ST, RATIO, LRN, SPLIT) \
     k_sweep_b<ST, RATIO, LRN, SPLIT><<<nb, 128, 0, s>>>(c, cellstart, pos, press, vel_out, gc, ncount, nlist,        \

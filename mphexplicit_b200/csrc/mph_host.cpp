@@ -74,7 +74,7 @@ struct StepGraphs {
     const int* nlist = nullptr;
     const int* nlist_s = nullptr;
     int launches_step = 0, launches_rebuild = 0;  // kernels per step and per rebuild
-    bool enabled = true;
+    bool enabled = false;  // mph_set_step_graphs
 };
 
 // mph_step_read_state: the copy stream (packs and device-to-host copies), its

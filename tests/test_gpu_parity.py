@@ -296,11 +296,13 @@ INFO_KEYS = ("step", "rebuild_count", "time", "max_neighbor_count", "neighbor_ca
 
 @pytest.mark.parametrize("name", ["dam_break_small", "two_fluid_small", "moving_walls", "droplet_2d", "bridge"])
 def test_step_graphs_match_host_path(name):
-    """Several FP64 steps per mph_step run as graph launches whose conditional
-    nodes take the rebuild test on the device; the host path (one flag read
-    per step) gives the same bits, rebuilds, step count and time."""
+    """With mph_set_step_graphs, several FP64 steps per mph_step run as graph
+    launches whose conditional nodes take the rebuild test on the device; the
+    host path (one flag read per step) gives the same bits, rebuilds, step
+    count and time."""
     case = GoldenCase(name)
     a, b = solver_for(case), solver_for(case)
+    a.set_step_graphs(True)
     b.set_step_graphs(False)
     done = 0
     for m in (1, 2, 7, 13, case.steps):
@@ -333,6 +335,7 @@ def test_step_graphs_grow_the_table_mid_batch():
     sc = scenes.droplet_2d(n=20, seed=9)
     a = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
     b = M.Solver(sc.params, sc.header, sc.type, sc.xyz, sc.vel, dim=2)
+    a.set_step_graphs(True)
     b.set_step_graphs(False)
     cap0 = a.info()["neighbor_capacity"]
     for s in (a, b):
