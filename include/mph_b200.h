@@ -245,6 +245,13 @@ int mph_step(mph_ctx* ctx, int nsteps);
  * per-step read costs about what the graph's control kernels do). */
 int mph_set_step_graphs(mph_ctx* ctx, int enable);
 
+/* The FP64 (and learned) form's pair sweeps: 0 (the default) by size, one
+ * warp per particle up to 40,000 particles in 3-D and 20,000 in 2-D, one
+ * thread per particle above; 1 always a thread per particle; 2 always a warp
+ * per particle.  The same bits either way (the warp's lanes compute the terms
+ * of 32 list entries, one lane per sum adds them in list order). */
+int mph_set_sweep_layout(mph_ctx* ctx, int layout);
+
 /* Wait for the context's stream and report any device-side error flag. */
 int mph_synchronize(mph_ctx* ctx);
 

@@ -194,6 +194,7 @@ SIGNATURES = {
     "mph_set_state": (_I, [_P, _dp, _dp]),
     "mph_step_read_state": (_I, [_P, C.c_int, _dp, _dp]),
     "mph_set_step_graphs": (_I, [_P, C.c_int]),
+    "mph_set_sweep_layout": (_I, [_P, C.c_int]),
     "mph_get_fields": (_I, [_P, _dp, _dp, _dp, _dp]),
     "mph_get_cells": (_I, [_P, _ip, _ip, _ip, _ip, _ip]),
     "mph_get_neighbors": (_I, [_P, C.POINTER(C.c_longlong), _ip, C.c_longlong]),

@@ -994,6 +994,7 @@ inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 #define MPH_WARP_SWEEP_MAX_N_2D 20000
 #endif
 inline bool use_warp_sweeps(const SimConst& c) {
+    if (c.sweep_layout != 0) return c.sweep_layout == 2;
     return c.n <= (c.dim == 2 ? MPH_WARP_SWEEP_MAX_N_2D : MPH_WARP_SWEEP_MAX_N);
 }
 

@@ -1200,6 +1200,14 @@ extern "C" int mph_step(mph_ctx* ctx, int nsteps) {
     return step_fp64(ctx, nsteps);
 }
 
+extern "C" int mph_set_sweep_layout(mph_ctx* ctx, int layout) {
+    if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
+    if (layout < 0 || layout > 2) return fail(ctx, MPH_ERR_ARG, "layout must be 0, 1 or 2");
+    ctx->sc.sweep_layout = layout;
+    drop_step_graphs(ctx);  // they hold the constants by value
+    return MPH_OK;
+}
+
 extern "C" int mph_set_step_graphs(mph_ctx* ctx, int enable) {
     if (!ctx) return fail(nullptr, MPH_ERR_ARG, "ctx is NULL");
     ctx->sg.enabled = enable != 0;

@@ -41,6 +41,7 @@ struct SimConst {
     double visc_c;                     // 8 (2-D) or 10 (3-D)
     double inv_r2g;                    // RN(1/R2g)
     int rg_eq_ra, rv_eq_ra;            // radii equal: r/h shared
+    int sweep_layout;                  // FP64 sweeps: 0 by size, 1 thread per particle, 2 warp per particle
     // visc_c * muij per type pair, muij = 2*(mu_i*mu_j)/(mu_i+mu_j) (main.cpp:1968)
     double visc_mu[MPH_TYPE_COUNT][MPH_TYPE_COUNT];
     double shift_thr;                  // 0.5*MARGIN*0.5*MARGIN

@@ -312,6 +312,11 @@ class Solver:
         _check(self._lib.mph_get_state(self._ctx, None, None, _dp(xyz), _dp(vel), None, None, None, None, None),
                self._ctx)
 
+    def set_sweep_layout(self, layout: str) -> None:
+        """FP64 pair sweeps: "auto" (by size), "thread" or "warp" per particle."""
+        code = {"auto": 0, "thread": 1, "warp": 2}[layout]
+        _check(self._lib.mph_set_sweep_layout(self._ctx, code), self._ctx)
+
     def set_step_graphs(self, enable: bool) -> None:
         """Graph launches for several FP64 steps (default) or the host path."""
         _check(self._lib.mph_set_step_graphs(self._ctx, 1 if enable else 0), self._ctx)

@@ -23,14 +23,20 @@ from tests.common import (CASES, CELL_KEYS, FIELD_KEYS, LONG_CASES, STATE_KEYS, 
 pytestmark = pytest.mark.gpu
 
 
-def solver_for(case: GoldenCase, mode="fp64") -> M.Solver:
-    return M.Solver.from_files(case.data, case.grid, dim=case.dim, mode=mode)
+def solver_for(case: GoldenCase, mode="fp64", layout="auto") -> M.Solver:
+    s = M.Solver.from_files(case.data, case.grid, dim=case.dim, mode=mode)
+    if layout != "auto":
+        s.set_sweep_layout(layout)
+    return s
 
 
+# The golden cases are small: "auto" runs the warp-per-particle sweeps on
+# them, "thread" the thread-per-particle ones the large scenes use.
+@pytest.mark.parametrize("layout", ["auto", "thread"])
 @pytest.mark.parametrize("name", CASES)
-def test_fp64_matches_reference_golden(name):
+def test_fp64_matches_reference_golden(name, layout):
     case = GoldenCase(name)
-    s = solver_for(case)
+    s = solver_for(case, layout=layout)
     s.step(case.steps)
     s.synchronize()
     s.compute_virial()
@@ -53,13 +59,14 @@ def test_fp64_matches_reference_golden(name):
     s.close()
 
 
+@pytest.mark.parametrize("layout", ["auto", "thread"])
 @pytest.mark.parametrize("name", LONG_CASES)
-def test_fp64_matches_reference_golden_1000_steps(name):
+def test_fp64_matches_reference_golden_1000_steps(name, layout):
     """3-D, 1000 steps from inside the developed flow (dozens of neighbour
     rebuilds), against the reference's own arrays: bit for bit (stricter than
     the 1e-10 relative bound on the FP64 state)."""
     case = GoldenCase(name)
-    s = solver_for(case)
+    s = solver_for(case, layout=layout)
     s.step(case.steps)
     s.synchronize()
     s.compute_virial()
