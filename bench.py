@@ -506,6 +506,24 @@ def measure_two_fluid(args, rank):
                                                  np.linalg.norm(f["vel"][fl])),
                      "kernels_ms_per_step": {k: v[1] / steps for k, v in r["prof"].items()}}
     out["value"] = out["mixed"]["value"]
+    out["fp64_value"] = sc.n_fluid * steps / (f["ms"] / 1e3)
+    from oracle import ref_inputs as RI
+    if rank == 0 and RI.ref_available(3) and not args.no_cpu_baseline and args.two_fluid_ref_seconds > 0:
+        # the reference on the same column, a bounded sample (its start-up,
+        # reading 8.5 M particles and the first lists, is not timed)
+        cores = RI.host_cores()
+        with tempfile.TemporaryDirectory() as td:
+            d, g, nn, nf = RI.two_fluid_files(td, seed=rank, n=n)
+            r = RI.time_reference(d, g, 3, 0, 1000, cores["logical"], max_seconds=args.two_fluid_ref_seconds,
+                                  timeout=3600)
+        ref_value = nf * r["steps"] / r["seconds"]
+        out["reference"] = {"kind": "reference (oracle/_ref/ref_mph3d, the reference's Mph_gcc3d flags)",
+                            "value": ref_value, "threads": cores["logical"], "steps": r["steps"],
+                            "seconds": r["seconds"], "startup_seconds": r.get("startup_seconds"),
+                            "sample": "%d timed step(s) of the full column on %d OpenMP threads"
+                                      % (r["steps"], cores["logical"])}
+        out["fp64_vs_reference"] = out["fp64_value"] / ref_value
+        out["mixed_vs_reference"] = out["mixed"]["value"] / ref_value
     return out
 
 
@@ -789,6 +807,8 @@ def main():
     ap.add_argument("--output-files", type=int, default=5)
     ap.add_argument("--two-fluid-n", type=int, default=200, help="fluid particles per axis of the two-fluid column")
     ap.add_argument("--two-fluid-steps", type=int, default=500)
+    ap.add_argument("--two-fluid-ref-seconds", type=float, default=20.0,
+                    help="budget of the reference's timed sample on the two-fluid column (0: skip)")
     ap.add_argument("--batch-check", type=int, default=16, help="scenes checked against the FP64 form")
     ap.add_argument("--batch-cpu-scenes", type=int, default=16)
     ap.add_argument("--batch-cpu-steps", type=int, default=200)

@@ -8,7 +8,8 @@ the reference runs the reference's code and nothing of the product.
 * ``dam_break_arrays``: the seeded 3-D dam-break scene (fluid block of type 0 in
   the corner of a box closed by type-2 wall layers), the same arrays as the
   product's scene generator (a CPU test compares them element for element);
-  ``droplet_arrays``: the 2-D square droplet, likewise.
+  ``droplet_arrays`` and ``two_fluid_arrays``: the 2-D square droplet and the
+  two-fluid column, likewise.
 * ``write_data`` / ``write_grid``: the reference's *.data keys (readDataFile,
   source/main.cpp:502-521) and *.grid layout (readGridFile, main.cpp:541-640;
   the generator's writer, generator/generator.cpp:197-217).
@@ -105,6 +106,45 @@ def droplet_arrays(n=40, l0=0.004, seed=0, box=100.0, steps=1000, rho=1000.0, mu
     header = {"time": 0.0, "n": len(xyz), "l0": l0, "dmin": [-half * l0, -half * l0, -0.5 * l0],
               "dmax": [half * l0, half * l0, 0.5 * l0]}
     return params, header, np.zeros(len(xyz), np.int32), xyz, np.zeros_like(xyz)
+
+
+def two_fluid_arrays(n=200, l0=0.0025, walls=2, seed=0, steps=500, mu=0.01, sigma=0.05, c_sound=20.0, dt=1.0e-5,
+                     modes=4):
+    """(params dict, header dict, type, xyz, vel) of the two-fluid column: n^3
+    fluid, type 1 above an interface displaced by a seeded sum of cosine modes
+    of amplitude 2 l0 and type 0 below, densities 500 / 1000, closed walls
+    whose layers alternate types 2 and 3, gravity -9.81 z, surface tension."""
+    rng = np.random.default_rng(seed)
+    f = _lattice((n, n, n), l0)
+    L = n * l0
+    kx = rng.integers(1, 5, modes)
+    ky = rng.integers(1, 5, modes)
+    ph = rng.uniform(0, 2 * np.pi, (modes, 2))
+    amp = 2.0 * l0 / modes
+    z0 = 0.5 * L + sum(amp * np.cos(2 * np.pi * kx[m] * f[:, 0] / L + ph[m, 0]) *
+                       np.cos(2 * np.pi * ky[m] * f[:, 1] / L + ph[m, 1]) for m in range(modes))
+    ftype = np.where(f[:, 2] > z0, 1, 0).astype(np.int32)
+    f += rng.uniform(-0.01 * l0, 0.01 * l0, f.shape)
+    outer = n + 2 * walls
+    w = _lattice((outer,) * 3, l0, (-walls * l0,) * 3)
+    layer = np.max(np.stack([np.maximum(-w[:, d] / l0, w[:, d] / l0 - n) for d in range(3)]), axis=0)
+    keep = layer > 0
+    w = w[keep]
+    wtype = np.where(np.ceil(layer[keep]).astype(int) % 2 == 1, 2, 3).astype(np.int32)
+    xyz = np.concatenate([f, w])
+    typ = np.concatenate([ftype, wtype])
+    pad = _pad_for_cells(outer, 2.0)
+    rho = [500.0, 1000.0, 1000.0, 1000.0]
+    params = {"dt": dt, "output_interval": 1.0e30, "vtk_output_interval": 1.0e30, "end_time": dt * (steps - 0.5),
+              "radius_ratio_a": 3.5, "radius_ratio_p": 1.7, "radius_ratio_v": 3.5, "density": rho,
+              "bulk_modulus": [r * c_sound ** 2 for r in rho], "bulk_viscosity": [float(mu)] * 4,
+              "shear_viscosity": [float(mu)] * 4, "surface_tension": [float(sigma)] * 4,
+              "interaction_ratio": [[1.0] * 4 for _ in range(4)], "gravity": [0.0, 0.0, -9.81],
+              "wall_center": [[0.0] * 3 for _ in range(4)], "wall_velocity": [[0.0] * 3 for _ in range(4)],
+              "wall_omega": [[0.0] * 3 for _ in range(4)]}
+    header = {"time": 0.0, "n": len(xyz), "l0": l0, "dmin": [-(walls + pad) * l0] * 3,
+              "dmax": [(n + walls + pad) * l0] * 3}
+    return params, header, typ, xyz, np.zeros_like(xyz)
 
 
 def write_data(path: str, p: dict) -> None:
@@ -212,3 +252,13 @@ def droplet_files(td: str, seed: int = 0, **kw):
     write_data(d, p)
     write_grid(g, h, t, x, v)
     return d, g, int(h["n"])
+
+
+def two_fluid_files(td: str, seed: int = 0, **kw):
+    """Write the two-fluid column's *.data / *.grid into directory td; returns
+    (data path, grid path, particles, fluid)."""
+    p, h, t, x, v = two_fluid_arrays(seed=seed, **kw)
+    d, g = os.path.join(td, "column.data"), os.path.join(td, "column.grid")
+    write_data(d, p)
+    write_grid(g, h, t, x, v)
+    return d, g, int(h["n"]), int(np.count_nonzero(t < 2))

@@ -54,6 +54,20 @@ def test_droplet_arrays_equal_product_scene(n, seed):
         assert open(g1, "rb").read() == open(g2, "rb").read()
 
 
+def test_two_fluid_arrays_equal_product_scene():
+    sc = scenes.two_fluid_column(n=10, seed=4)
+    p, h, t, x, v = RI.two_fluid_arrays(n=10, seed=4)
+    assert np.array_equal(t, sc.type) and np.array_equal(x, sc.xyz) and np.array_equal(v, sc.vel)
+    with tempfile.TemporaryDirectory() as td:
+        d1, g1 = os.path.join(td, "a.data"), os.path.join(td, "a.grid")
+        d2, g2 = os.path.join(td, "b.data"), os.path.join(td, "b.grid")
+        sc.write(d1, g1)
+        RI.write_data(d2, p)
+        RI.write_grid(g2, h, t, x, v)
+        assert open(d1, "rb").read() == open(d2, "rb").read()
+        assert open(g1, "rb").read() == open(g2, "rb").read()
+
+
 def test_host_cores():
     c = RI.host_cores()
     assert c["logical"] >= 1 and 1 <= c["physical"] <= c["logical"]
