@@ -230,19 +230,20 @@ int mph_create(const mph_params* p, const mph_grid_header* h, int dim, int mode,
 
 /* Advance nsteps explicit steps: the loop body main.cpp:386-431 plus
  * Time += Dt (main.cpp:449).  No file output.  Returns when the steps are
- * done.  Each step the host reads the neighbour-rebuild test's flag after the
- * move (see mph_set_step_graphs for the alternative). */
+ * done.  Several FP64 steps run as one CUDA graph launch each, whose
+ * conditional nodes make the neighbour-rebuild test (in the move kernel's
+ * last block) and check a rebuilt list against its table on the device, with
+ * no host round trip until the end: the same kernels, so the same bits.  A
+ * list that outgrows its table ends the graph launches after that step's
+ * reorder; the host grows the table and finishes the steps.  One step, the
+ * mixed and learned forms, profiling on (mph_profile_enable), or graphs off:
+ * the host reads the rebuild flag after each step's move. */
 int mph_step(mph_ctx* ctx, int nsteps);
 
-/* enable == 1: mph_step of several FP64 steps runs one CUDA graph launch per
- * step, whose conditional nodes make the rebuild test (and check the rebuilt
- * list against its table) on the device, with no host round trip until the
- * end; the same kernels, so the same bits.  A list that outgrows its table
- * ends the graph launches after that step's reorder; the host grows the table
- * and finishes the steps.  With profiling on (mph_profile_enable) the host
- * path runs.  0 (the default): the host path.  Measured on one B200, scenes
- * of 1.6 k to 2.8 M particles: within +-3 % of the host path either way (the
- * per-step read costs about what the graph's control kernels do). */
+/* enable == 0: mph_step takes the host path for every step; 1 (the
+ * default): graph launches for several FP64 steps.  Measured on one B200:
+ * 0.036 against 0.040 ms per step on a 1,600-particle droplet, 2-3 % on
+ * 10-20 k particles, within 1 % at 0.1-2.8 M particles. */
 int mph_set_step_graphs(mph_ctx* ctx, int enable);
 
 /* The FP64 (and learned) form's pair sweeps: 0 (the default) by size, one

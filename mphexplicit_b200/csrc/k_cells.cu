@@ -356,19 +356,8 @@ __global__ void k_unpack3(int n, const double* __restrict__ src, double4* __rest
 
 inline int blocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
-// Control kernels of the FP64 step graphs (one thread each): they set the
-// conditional nodes that take the place of the host's per-step decisions.
-__global__ void k_graph_gate(StepScalars* scal, cudaGraphConditionalHandle run) {
-    cudaGraphSetConditional(run, scal->stop ? 0u : 1u);
-}
-
-__global__ void k_graph_decide(StepScalars* scal, double thr, cudaGraphConditionalHandle rebuild) {
-    const double ms = __longlong_as_double((long long)scal->max_shift2_bits);
-    const bool r = ms > thr;  // neighborCalculation() == 1 (main.cpp:1102)
-    cudaGraphSetConditional(rebuild, r ? 1u : 0u);
-    if (r) scal->rebuilds_done += 1;
-}
-
+// Table check of a step graph's rebuild (one thread): a list longer than its
+// table stops the batch and skips this step's sweeps.
 __global__ void k_graph_list_check(StepScalars* scal, int cap, int cap_s, int short_list,
                                    cudaGraphConditionalHandle sweep) {
     if (scal->max_neighbors > cap || (short_list && scal->max_short > cap_s)) {
@@ -377,22 +366,12 @@ __global__ void k_graph_list_check(StepScalars* scal, int cap, int cap_s, int sh
     }
 }
 
-__global__ void k_graph_step_done(StepScalars* scal) { scal->steps_done += 1; }
-
 }  // namespace
 
-void launch_graph_gate(StepScalars* scal, cudaGraphConditionalHandle run, cudaStream_t s) {
-    k_graph_gate<<<1, 1, 0, s>>>(scal, run);
-}
-void launch_graph_decide(StepScalars* scal, double shift_thr, cudaGraphConditionalHandle rebuild,
-                         cudaStream_t s) {
-    k_graph_decide<<<1, 1, 0, s>>>(scal, shift_thr, rebuild);
-}
 void launch_graph_list_check(StepScalars* scal, int cap, int cap_s, int short_list,
                              cudaGraphConditionalHandle sweep, cudaStream_t s) {
     k_graph_list_check<<<1, 1, 0, s>>>(scal, cap, cap_s, short_list, sweep);
 }
-void launch_graph_step_done(StepScalars* scal, cudaStream_t s) { k_graph_step_done<<<1, 1, 0, s>>>(scal); }
 
 void launch_cell_index(const SimConst& c, const double4* pos, const int* type, int* keys, int* vals,
                        cudaStream_t s) {

@@ -93,12 +93,19 @@ __device__ __forceinline__ int type_of(const double4& p) { return (int)p.w; }
 
 // Convection (main.cpp:1605-1615), Wall (2013-2043), PeriodicBoundary
 // (2306-2317) and the displacement maximum of neighborCalculation (1086-1100).
+// GRAPH (a step graph's move): nothing to do once the batch stopped; the last
+// block to finish makes the rebuild test on the maximum (main.cpp:1102) and
+// sets the graph's conditionals, counts the step and clears the maximum for
+// the next step's move.
+template <bool GRAPH>
 __global__ void __launch_bounds__(256)
 k_move(SimConst c, const int* __restrict__ cellstart, double4* __restrict__ pos, double4* __restrict__ vel,
-       const double4* __restrict__ snap, const double* __restrict__ wall_center, StepScalars* __restrict__ scal) {
+       const double4* __restrict__ snap, const double* __restrict__ wall_center, StepScalars* __restrict__ scal,
+       cudaGraphConditionalHandle h_rebuild, cudaGraphConditionalHandle h_sweep) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool stopped = GRAPH && *reinterpret_cast<volatile int*>(&scal->stop) != 0;
     double s2 = 0.0;
-    if (i < c.n) {
+    if (i < c.n && !stopped) {
         const int nf = cellstart[c.tot], we = cellstart[2 * c.tot];
         double4 p = pos[i];
         if (i < nf) {
@@ -149,6 +156,20 @@ k_move(SimConst c, const int* __restrict__ cellstart, double4* __restrict__ pos,
         double m = red[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = red[w] > m ? red[w] : m;
         if (m > 0.0) atomicMax(&scal->max_shift2_bits, (unsigned long long)__double_as_longlong(m));
+        if (GRAPH) {
+            __threadfence();
+            if (atomicAdd(&scal->blocks_done, 1u) == gridDim.x - 1) {  // the last block
+                __threadfence();
+                const unsigned long long bits = atomicAdd(&scal->max_shift2_bits, 0ull);
+                const bool rebuild = !stopped && __longlong_as_double((long long)bits) > c.shift_thr;
+                cudaGraphSetConditional(h_rebuild, rebuild ? 1u : 0u);
+                cudaGraphSetConditional(h_sweep, stopped ? 0u : 1u);
+                if (rebuild) scal->rebuilds_done += 1;
+                if (!stopped) scal->steps_done += 1;
+                scal->max_shift2_bits = 0ull;
+                scal->blocks_done = 0u;
+            }
+        }
     }
 }
 
@@ -1194,7 +1215,14 @@ k_force_compare(int nf, const double4* __restrict__ fa, const double4* __restric
 
 void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel, const double4* snap,
                  const double* wall_center, StepScalars* scal, cudaStream_t s) {
-    k_move<<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, snap, wall_center, scal);
+    k_move<false><<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, snap, wall_center, scal, 0, 0);
+}
+
+void launch_move_graph(const SimConst& c, const int* cellstart, double4* pos, double4* vel, const double4* snap,
+                       const double* wall_center, StepScalars* scal, cudaGraphConditionalHandle rebuild,
+                       cudaGraphConditionalHandle sweep, cudaStream_t s) {
+    k_move<true><<<blocks(c.n, 256), 256, 0, s>>>(c, cellstart, pos, vel, snap, wall_center, scal, rebuild,
+                                                  sweep);
 }
 
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos, const double4* vel,

@@ -66,15 +66,16 @@ struct LearnedState {
 
 // mph_step in the FP64 form for more than one step: one executable graph per
 // parity of the velocity ping-pong, replayed once per step, whose conditional
-// nodes take the host's per-step decisions (the rebuild test and the table
-// check); made for the buffers and table capacities they were captured with.
+// nodes take the host's per-step decisions (the rebuild test, made by the
+// move kernel's last block, and the table check); made for the buffers and
+// table capacities they were captured with.
 struct StepGraphs {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};  // by the vcur of the step
     int cur = -1, cap = -1, cap_s = -1;
     const int* nlist = nullptr;
     const int* nlist_s = nullptr;
     int launches_step = 0, launches_rebuild = 0;  // kernels per step and per rebuild
-    bool enabled = false;  // mph_set_step_graphs
+    bool enabled = true;  // mph_set_step_graphs
 };
 
 // mph_step_read_state: the copy stream (packs and device-to-host copies), its
@@ -749,11 +750,11 @@ static int add_if_node(mph_ctx* ctx, cudaStream_t st, cudaGraphConditionalHandle
 }
 
 // Captures one FP64 step for vcur == v:
-//   gate -> IF run { memset, move, decide -> IF rebuild { cell index, bitonic
-//   sort, cell ranges, reorder (then copied back into the buffers this graph
-//   holds), pos32, neighbour list, table check }, IF sweep { sweep A, force
-//   sweep, step done } }
-// The same kernels with the same arguments as step_fp64, so the same bits.
+//   move (its last block makes the rebuild test and sets both conditionals)
+//   -> IF rebuild { cell index, bitonic sort, cell ranges, reorder (then copied
+//   back into the buffers this graph holds), pos32, neighbour list, table
+//   check } -> IF sweep { sweep A, force sweep }
+// The kernels and arguments of step_fp64, so the same bits.
 static int capture_step(mph_ctx* ctx, int v, cudaGraphExec_t* out, int* launches_step, int* launches_rebuild) {
     mph::DevFP64& d = ctx->d;
     const SimConst& s = ctx->sc;
@@ -762,8 +763,8 @@ static int capture_step(mph_ctx* ctx, int v, cudaGraphExec_t* out, int* launches
     const size_t n = (size_t)ctx->n;
     const bool sl = uses_short_list(ctx);
     const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-    cudaGraph_t g = nullptr, g_run = nullptr, g_reb = nullptr, g_sw = nullptr;
-    cudaGraphConditionalHandle h_run = 0, h_reb = 0, h_sw = 0;
+    cudaGraph_t g = nullptr, g_reb = nullptr, g_sw = nullptr;
+    cudaGraphConditionalHandle h_reb = 0, h_sw = 0;
     int rc = MPH_OK;
     auto ck = [&](cudaError_t e) {
         if (e != cudaSuccess && rc == MPH_OK)
@@ -776,20 +777,11 @@ static int capture_step(mph_ctx* ctx, int v, cudaGraphExec_t* out, int* launches
         ck(cudaGetLastError());
     };
     int ls = 0, lr = 0;
-    if (ck(cudaGraphCreate(&g, 0)) && ck(cudaGraphConditionalHandleCreate(&h_run, g, 0, 0)) &&
+    if (ck(cudaGraphCreate(&g, 0)) && ck(cudaGraphConditionalHandleCreate(&h_reb, g, 0, 0)) &&
+        ck(cudaGraphConditionalHandleCreate(&h_sw, g, 0, 0)) &&
         ck(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, mode))) {
-        mph::launch_graph_gate(d.scal, h_run, st);
-        ++ls;
-        if (rc == MPH_OK) rc = add_if_node(ctx, st, h_run, &g_run);
-        end_capture();
-    }
-    if (rc == MPH_OK && ck(cudaGraphConditionalHandleCreate(&h_reb, g_run, 0, 0)) &&
-        ck(cudaGraphConditionalHandleCreate(&h_sw, g_run, 1, cudaGraphCondAssignDefault)) &&
-        ck(cudaStreamBeginCaptureToGraph(st, g_run, nullptr, nullptr, 0, mode))) {
-        ck(cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
-        mph::launch_move(s, d.cellstart, d.pos[a], d.vel[va], d.snap, d.wall_center, d.scal, st);
-        mph::launch_graph_decide(d.scal, s.shift_thr, h_reb, st);
-        ls += 2;
+        mph::launch_move_graph(s, d.cellstart, d.pos[a], d.vel[va], d.snap, d.wall_center, d.scal, h_reb, h_sw, st);
+        ls += 1;
         if (rc == MPH_OK) rc = add_if_node(ctx, st, h_reb, &g_reb);
         if (rc == MPH_OK) rc = add_if_node(ctx, st, h_sw, &g_sw);
         end_capture();
@@ -819,8 +811,7 @@ static int capture_step(mph_ctx* ctx, int v, cudaGraphExec_t* out, int* launches
         mph::launch_sweep_b(s, d.cellstart, d.pos[a], d.vel[va], d.vel[vb], d.press, d.gc, d.ncount, d.nlist,
                             sl ? d.ncount_s : nullptr, sl ? d.nlist_s : nullptr, d.force, d.scal, st, nullptr,
                             nullptr, nullptr, 1);
-        mph::launch_graph_step_done(d.scal, st);
-        ls += 3;
+        ls += 2;
         end_capture();
     }
     if (rc == MPH_OK) ck(cudaGraphInstantiate(out, g, 0));
@@ -876,16 +867,21 @@ static int step_fp64_graphs(mph_ctx* ctx, int nsteps) {
     mph::DevFP64& d = ctx->d;
     cudaStream_t st = ctx->stream;
     TRY(ensure_step_graphs(ctx));
-    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->stop, 0, 3 * sizeof(int), st));  // stop, steps_done, rebuilds_done
+    // the graphs' move accumulates into a cleared maximum and clears it again
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->max_shift2_bits, 0, sizeof(unsigned long long), st));
+    CUDA_TRY(ctx, cudaMemsetAsync(&d.scal->stop, 0, 4 * sizeof(int), st));  // stop, steps, rebuilds, blocks
     for (int k = 0; k < nsteps; ++k) CUDA_TRY(ctx, cudaGraphLaunch(G.exec[(d.vcur + k) & 1], st));
     TRY(read_scalars(ctx));
     const StepScalars& h = *ctx->h_scal;
-    const int done = h.steps_done, reb = h.rebuilds_done, stopped = h.stop;
+    const int stopped = h.stop, reb = h.rebuilds_done;
+    const int done = h.steps_done - stopped;  // steps moved, less the one whose list overflowed
     for (int k = 0; k < done; ++k) ctx->time += ctx->p.dt;  // main.cpp:449, one step at a time
     ctx->step += done;
     if (done & 1) d.vcur = 1 - d.vcur;
     ctx->rebuilds += reb;
     ctx->launches += (long long)G.launches_step * (done + stopped) + (long long)G.launches_rebuild * reb;
+    static_assert(offsetof(StepScalars, blocks_done) == offsetof(StepScalars, stop) + 3 * sizeof(int),
+                  "stop, steps_done, rebuilds_done and blocks_done are cleared together");
     if (reb > 0) {
         ctx->max_neighbors = h.max_neighbors;
         ctx->lrn.edges_valid = false;

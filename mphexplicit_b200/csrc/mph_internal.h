@@ -62,9 +62,10 @@ struct StepScalars {
     int rebuild;                         // decision of the last move kernel
     int max_short, max_long;             // longest short / long part (mixed table)
     int stop;                            // step graphs: a list overflowed, the later steps skip
-    int steps_done;                      // step graphs: steps completed in this batch
+    int steps_done;                      // step graphs: steps started (moved) in this batch
     int rebuilds_done;                   // step graphs: rebuilds started in this batch
-    int pad[6];
+    unsigned blocks_done;                // step graphs: move blocks finished in this launch
+    int pad[5];
 };
 
 enum : int {
@@ -135,16 +136,17 @@ void launch_neighbor_list(const SimConst& c, const double4* pos, const float4* p
                           StepScalars* scal, cudaStream_t s);
 void launch_pack3(int n, const double4* src, double* dst, cudaStream_t s);
 
-// ---- step graphs (FP64 form; the control kernels of k_cells.cu) ----------
-// gate: run = 1 unless an earlier step of the batch stopped
-void launch_graph_gate(StepScalars* scal, cudaGraphConditionalHandle run, cudaStream_t s);
-// rebuild test of main.cpp:1102 on the move kernel's maximum shift
-void launch_graph_decide(StepScalars* scal, double shift_thr, cudaGraphConditionalHandle rebuild,
-                         cudaStream_t s);
+// ---- step graphs (FP64 form) ------------------------------------------------
 // after a list build: a list longer than its table stops the batch (sweep = 0)
 void launch_graph_list_check(StepScalars* scal, int cap, int cap_s, int short_list,
                              cudaGraphConditionalHandle sweep, cudaStream_t s);
-void launch_graph_step_done(StepScalars* scal, cudaStream_t s);
+// the move of a step graph (k_fp64.cu): as launch_move, and its last block
+// makes the rebuild test of main.cpp:1102 (rebuild = 1 when it fires; sweep =
+// 1 unless the batch stopped, when the move does nothing), counts the step
+// and clears the maximum shift for the next step
+void launch_move_graph(const SimConst& c, const int* cellstart, double4* pos, double4* vel, const double4* snap,
+                       const double* wall_center, StepScalars* scal, cudaGraphConditionalHandle rebuild,
+                       cudaGraphConditionalHandle sweep, cudaStream_t s);
 void launch_unpack3(int n, const double* src, double4* dst, const int* type, cudaStream_t s);
 
 // ---- kernel launchers (k_fp64.cu) -----------------------------------------
