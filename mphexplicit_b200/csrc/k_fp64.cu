@@ -19,14 +19,14 @@
 // Resident 128-thread blocks per SM the sweeps are compiled for (register cap
 // 65536 / (128 * blocks)); latency hiding vs. spills, set by measurement on
 // the full dam break.  Both sweeps keep the next neighbour's records in
-// flight: sweep A at 7 (72 registers; at 8 it spills), the force sweep at 5
-// (90 registers, no spills: 3.46 ms against 3.69 ms without the prefetch at 7
-// blocks, 4.21 ms with it at 6, before its pressure loop was split off).
+// flight: sweep A at 7 (72 registers; at 8 it spills), the force sweep at 6
+// (80 registers, a few spills outside the neighbour loops: 3.08 ms against
+// 3.13 ms at 5 blocks and 3.16 ms at 4, with the pressure loop split off).
 #ifndef MPH_SWEEP_MINB
 #define MPH_SWEEP_MINB 7
 #endif
 #ifndef MPH_SWEEPB_MINB
-#define MPH_SWEEPB_MINB 5
+#define MPH_SWEEPB_MINB 6
 #endif
 // The surface-tension variants hold more live values per pair; at the
 // bounds above they spilled (140 B in the force sweep) and ran the 8.5 M
