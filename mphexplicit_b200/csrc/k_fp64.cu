@@ -32,7 +32,8 @@
 // bounds above they spilled (140 B in the force sweep) and ran the 8.5 M
 // particle two-fluid column's step at 40.6 + 13.9 ms.  Measured on that
 // column: the force sweep 26.7 ms at 4 blocks (no spills) and 29.6 ms at 3,
-// sweep A 12.5 ms at 5 (13.3 at 6); results bit-identical.
+// sweep A 12.5 ms at 5 (13.3 at 6); results bit-identical.  With the pressure
+// loops over the short sublist (SPLIT): 26.0 and 10.2 ms.
 #ifndef MPH_SWEEP_MINB_ST
 #define MPH_SWEEP_MINB_ST 5
 #endif
@@ -195,10 +196,15 @@ __device__ __forceinline__ double s_dwv(const SimConst& c, double q) { return c.
 // terms are not evaluated), so the step leaves them to k_density_a, run only
 // when they are read, and visits only the short sublist (the pairs that can
 // lie within RadiusP, in list order).
-template <bool ST, bool RATIO, bool DA>
+// SPLIT (with surface tension): DensityP and DivergenceP over the short
+// sublist (ncount_p, nlist_p: the list's entries within RadiusP+MARGIN, in list
+// order, so the same sums), DensityA and GravityCenter over the list; the
+// pressure block then no longer runs with most lanes masked off.
+template <bool ST, bool RATIO, bool DA, bool SPLIT>
 __global__ void __launch_bounds__(128, ST ? MPH_SWEEP_MINB_ST : MPH_SWEEP_MINB)
 k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict__ vel,
-          const int* __restrict__ ncount, const int* __restrict__ nlist, double* __restrict__ dens_a,
+          const int* __restrict__ ncount, const int* __restrict__ nlist, const int* __restrict__ ncount_p,
+          const int* __restrict__ nlist_p, double* __restrict__ dens_a,
           double* __restrict__ strain_p, double* __restrict__ div_p, double4* __restrict__ velp,
           double4* __restrict__ gcpa, double* __restrict__ wall_center) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -216,6 +222,41 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
     const size_t n = (size_t)c.n;
     double sum_a = 0.0, sum_p = 0.0, sum_d = 0.0;
     double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+    if (SPLIT) {  // DensityP, DivergenceP over the short sublist (main.cpp:1831-1896)
+        const int cs = ncount_p[i];
+        const int* lq = nlist_p + i;
+        int q1 = cs > 0 ? __ldg(lq) : i;
+        int q2 = cs > 1 ? __ldg(lq + n) : i;
+        lq += 2 * n;
+        double4 qn = pos[q1], qv = vel[q1];
+        for (int k = 0; k < cs; ++k) {
+            const int j = q1;
+            const double4 pj = qn;
+            const double4 vjn = qv;
+            q1 = q2;
+            if (k + 2 < cs) q2 = __ldg(lq);
+            lq += n;
+            if (k + 1 < cs) {
+                qn = pos[q1];
+                qv = vel[q1];
+            }
+            if (j == i) continue;
+            double x[3];
+            disp(c, pi, pj, x);
+            const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+            if (!(r2 <= c.rp2)) continue;
+            const double r = sqrt(r2);
+            const double qp = div_rs(r, c.rp, c.inv_rp);
+            sum_p += s_wp(c, qp);
+            const double dw = s_dwp(c, qp);
+            const double ri = __drcp_rn(r);
+            const double e0 = div_rs(x[0], r, ri), e1 = div_rs(x[1], r, ri), e2 = div_rs(x[2], r, ri);
+            const double u0 = vjn.x - vi.x, u1 = vjn.y - vi.y, u2 = vjn.z - vi.z;
+            sum_d -= u0 * e0 * dw;
+            sum_d -= u1 * e1 * dw;
+            sum_d -= u2 * e2 * dw;
+        }
+    }
     // indices two entries ahead, the neighbour's position and velocity one ahead
     const int* lp = nlist + i;
     int j1 = cnt > 0 ? __ldg(lp) : i;
@@ -240,7 +281,7 @@ k_sweep_a(SimConst c, const double4* __restrict__ pos, const double4* __restrict
         // R*R - r2 >= 0 (main.cpp:1683 and the other density sums) is r2 <= R*R:
         // with gradual underflow a - b is zero only when a == b, and its sign exact
         const bool in_a = DA && (r2 <= c.ra2);
-        const bool in_p = r2 <= c.rp2;
+        const bool in_p = !SPLIT && r2 <= c.rp2;
         const bool in_g = ST && (r2 <= c.rg2);
         if (!(in_a || in_p || in_g)) continue;
         const double r = sqrt(r2);
@@ -1232,17 +1273,26 @@ void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
     (void)cellstart;
     const bool warp = use_warp_sweeps(c);
     const int nb = warp ? blocks(c.n, kWarpSweepWarps) : (blocks(c.n, 128) > 0 ? blocks(c.n, 128) : 1);
-#define SWEEP_A(ST, RATIO, CNT, LIST)                                                                             \
+    // with surface tension the list (DensityA, GravityCenter) and, when there
+    // is one, the short sublist (DensityP, DivergenceP); without, the short
+    // sublist alone
+    const bool split = c.has_st && nlist_s != nullptr;
+#define SWEEP_A(ST, RATIO, SPLIT, CNT, LIST)                                                                      \
     if (warp)                                                                                                     \
         k_sweep_a_w<ST, RATIO, ST><<<nb, 32 * kWarpSweepWarps, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p,  \
                                                                        div_p, press, gc, wall_center);            \
     else                                                                                                          \
-        k_sweep_a<ST, RATIO, ST><<<nb, 128, 0, s>>>(c, pos, vel, CNT, LIST, dens_a, strain_p, div_p, press, gc,   \
-                                                    wall_center)
+        k_sweep_a<ST, RATIO, ST, SPLIT><<<nb, 128, 0, s>>>(c, pos, vel, CNT, LIST, ncount_s, nlist_s, dens_a,     \
+                                                           strain_p, div_p, press, gc, wall_center)
     if (c.has_st) {
-        if (c.ratio_all_one) SWEEP_A(true, false, ncount, nlist); else SWEEP_A(true, true, ncount, nlist);
+        if (split) {
+            if (c.ratio_all_one) SWEEP_A(true, false, true, ncount, nlist); else SWEEP_A(true, true, true, ncount, nlist);
+        } else {
+            if (c.ratio_all_one) SWEEP_A(true, false, false, ncount, nlist); else SWEEP_A(true, true, false, ncount, nlist);
+        }
     } else {
-        if (c.ratio_all_one) SWEEP_A(false, false, ncount_s, nlist_s); else SWEEP_A(false, true, ncount_s, nlist_s);
+        if (c.ratio_all_one) SWEEP_A(false, false, false, ncount_s, nlist_s);
+        else SWEEP_A(false, true, false, ncount_s, nlist_s);
     }
 #undef SWEEP_A
 }
@@ -1284,7 +1334,7 @@ void launch_sweep_b(const SimConst& c, const int* cellstart, const double4* pos,
                                                         i0, i1, vel_host)
 #define SWEEP_B2(ST, RATIO)                                             \
     if (eforce) SWEEP_B(ST, RATIO, true, false);                        \
-    else if (!ST && nlist_s) SWEEP_B(ST, RATIO, false, !ST);            \
+    else if (nlist_s) SWEEP_B(ST, RATIO, false, true);                  \
     else SWEEP_B(ST, RATIO, false, false)
     if (c.has_st) {
         if (c.ratio_all_one) { SWEEP_B2(true, false); } else { SWEEP_B2(true, true); }

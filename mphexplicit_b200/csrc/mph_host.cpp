@@ -465,8 +465,12 @@ static int grow_table(mph_ctx* ctx, int need, int** table, int* capacity) {
 
 static int grow_list(mph_ctx* ctx, int need) { return grow_table(ctx, need, &ctx->d.nlist, &ctx->d.cap); }
 
-// The short sublist serves sweep A when there is no surface tension.
-static bool uses_short_list(const mph_ctx* ctx) { return !ctx->sc.has_st; }
+// The short sublist (the list's entries within RadiusP+MARGIN, in list order)
+// serves the pressure loops of both sweeps, with and without surface tension.
+static bool uses_short_list(const mph_ctx* ctx) {
+    (void)ctx;
+    return true;
+}
 
 // calculateCellParticle + calculateNeighbor (main.cpp:1111-1596).
 static int build_lists(mph_ctx* ctx);
