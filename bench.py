@@ -783,6 +783,9 @@ def measure_form(args, sc, mode, world, gpu_index, with_e2e):
     return out
 
 
+DEFAULT_FORMS = "fp64,mixed,mixed_p64,mixed_walk,learned,batch,two_fluid,droplet,output"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -796,8 +799,10 @@ def main():
     ap.add_argument("--scene", default="dam", choices=sorted(SCENES))
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--droplet-steps", type=int, default=1000, help="steps of the 2-D droplet (config 1)")
-    ap.add_argument("--forms", default="fp64,mixed,mixed_p64,mixed_walk,learned,batch,two_fluid,droplet,output",
-                    help="forms to measure (comma list); the headline --mode must be among them for a full line")
+    ap.add_argument("--forms", default=None,
+                    help="forms to measure (comma list; the headline --mode must be among them for a full line); "
+                         "default: all of " + DEFAULT_FORMS + " on one GPU, the headline form alone on several "
+                         "(the replicas' scaling line, the GPUs held for its timed steps only)")
     ap.add_argument("--learned-fluid", default="80,80,160", help="fluid block of the learned form's dam break")
     ap.add_argument("--learned-steps", type=int, default=1000)
     ap.add_argument("--learn-steps", type=int, default=2000, help="FP64 steps of training data")
@@ -840,7 +845,8 @@ def main():
     if cvd and "," not in cvd and cvd.isdigit():
         gpu_index = int(cvd)
     sc = make_scene(args, rank)
-    wanted = [args.mode] if args.only else [f.strip() for f in args.forms.split(",") if f.strip()]
+    forms_arg = args.forms if args.forms is not None else (DEFAULT_FORMS if world == 1 else args.mode)
+    wanted = [args.mode] if args.only else [f.strip() for f in forms_arg.split(",") if f.strip()]
     modes = [m for m in ("fp64", "mixed", "mixed_p64", "mixed_walk") if m in wanted]
     res = {m: measure_form(args, sc, m, world, gpu_index, with_e2e=(m == args.mode)) for m in modes}
     forms = {}
