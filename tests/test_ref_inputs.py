@@ -82,3 +82,21 @@ def test_time_reference_forced_rebuild():
         assert r["particles"] == n and r["fluid"] == nf
         r = RI.time_reference(d, g, 3, 0, 2, 1)
         assert r["rebuilds"] == 0
+
+
+@pytest.mark.skipif(not RI.ref_available(2), reason="reference build absent")
+def test_time_reference_droplet_2d():
+    """The reference's 2-D build steps the droplet the bench times it on."""
+    with tempfile.TemporaryDirectory() as td:
+        d, g, n = RI.droplet_files(td, n=12, seed=1)
+        r = RI.time_reference(d, g, 2, 1, 5, 1)
+        assert r["steps"] == 5 and r["particles"] == n == 144 and r["seconds"] > 0.0
+
+
+@pytest.mark.skipif(not RI.ref_available(3), reason="reference build absent")
+def test_time_reference_two_fluid_column():
+    """... and the two-fluid column (scaled down)."""
+    with tempfile.TemporaryDirectory() as td:
+        d, g, n, nf = RI.two_fluid_files(td, n=8, seed=2)
+        r = RI.time_reference(d, g, 3, 0, 2, 2)
+        assert r["steps"] == 2 and r["particles"] == n and r["fluid"] == nf == 512
