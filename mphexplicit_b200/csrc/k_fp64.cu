@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(128) k_density_a(SimConst c, const double4* __
 // terms are not evaluated; fluid particle i adds instead the sum of its
 // edge-MLP pair forces eforce[eoff[i] .. eoff[i+1]) (FP32, in edge order),
 // which is also stored in lsum[i].
-// SPLIT (no surface tension, not learned): the PressureP force visits only
+// SPLIT (not learned): the PressureP force visits only
 // pairs within RadiusP, all of which are in the short sublist, in list order
 // (the argument of k_neighbor_list), so that sum runs as its own loop over the
 // short sublist and the main loop carries ViscosityV alone.  The terms and

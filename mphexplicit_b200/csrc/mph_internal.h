@@ -97,7 +97,7 @@ struct DevFP64 {
     int* ncount = nullptr;                  // NeighborCount
     int* nlist = nullptr;                   // [cap][n] column-major list
     int cap = 0;
-    int* ncount_s = nullptr;                // short sublist (no surface tension): the entries
+    int* ncount_s = nullptr;                // short sublist: the entries
     int* nlist_s = nullptr;                 // within rs2, in list order, [cap_s][n]
     int cap_s = 0;
     double* wall_center = nullptr;          // [4][3], advanced on the device
@@ -153,8 +153,8 @@ void launch_unpack3(int n, const double* src, double4* dst, const int* type, cud
 void launch_move(const SimConst& c, const int* cellstart, double4* pos, double4* vel,
                  const double4* snap, const double* wall_center, StepScalars* scal,
                  cudaStream_t s);
-// Without surface tension sweep A visits the short sublist (ncount_s,
-// nlist_s); with it, the whole list.
+// Sweep A's DensityP and DivergenceP visit the short sublist (ncount_s,
+// nlist_s); with surface tension DensityA and GravityCenter the whole list.
 void launch_sweep_a(const SimConst& c, const int* cellstart, const double4* pos,
                     const double4* vel, const int* ncount, const int* nlist, const int* ncount_s,
                     const int* nlist_s, double* dens_a, double* strain_p, double* div_p, double4* press,
@@ -168,8 +168,8 @@ void launch_density_a(const SimConst& c, const double4* pos, const int* ncount, 
 // needs only the pairs within RadiusP, so the short sublist may be passed).
 // part: 0 every particle; 1 the fluid (walls copy their velocity, their
 // force is not written); 2 the walls' forces alone (vel_out unused).
-// ncount_s / nlist_s (no surface tension, not learned): the short sublist,
-// over which the PressureP force runs as its own loop (same result).
+// ncount_s / nlist_s (not learned): the short sublist, over which the
+// PressureP force runs as its own loop (same result).
 // [i0, i1): the particles (sorted order) this launch computes; i1 < 0 means
 // all n.  Every particle's result depends on the inputs alone, so a sweep
 // split into ranges gives the same bits as one launch.  vel_host (part 1): a
