@@ -181,6 +181,7 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
                 const int* __restrict__ cellstart, int* __restrict__ ncount, int* __restrict__ nlist, int cap,
                 int* __restrict__ ncount_s, int* __restrict__ nlist_s, int cap_s, StepScalars* __restrict__ scal) {
     __shared__ float4 cand[kListWarps][32];
+    __shared__ int4 sten[kListWarps][27];  // the stencil in visiting order: cell, FP32 image offsets
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int key = blockIdx.x * kListWarps + wib;  // home key in [0, 2*tot)
     if (key >= 2 * c.tot) return;                   // whole warp
@@ -205,6 +206,18 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
         off = raw < 0 ? -pf.width[d] : (raw >= c.cc[d] ? pf.width[d] : 0.0f);
         return ((ic[d] - c.range[d] + s_) % c.cc[d] + c.cc[d]) % c.cc[d];
     };
+    // lane s < w0*w1*w2 computes stencil slot s of the loop order of
+    // main.cpp:1356-1392 (x outer, z inner), once for all the key's chunks
+    const int nsl = w[0] * w[1] * w[2];  // at most 27: range <= 1 on every axis
+    if (lane < nsl) {
+        const int a0 = lane / (w[1] * w[2]), a1 = (lane / w[2]) % w[1], a2 = lane % w[2];
+        float gx, gy, gz;
+        const int cx = slot(0, (jmin[0] + a0) % w[0], gx), cy = slot(1, (jmin[1] + a1) % w[1], gy),
+                  cz = slot(2, (jmin[2] + a2) % w[2], gz);
+        sten[wib][lane] = make_int4(cell_id(c, cx, cy, cz), __float_as_int(gx), __float_as_int(gy),
+                                    __float_as_int(gz));
+    }
+    __syncwarp();
     const int wall_begin = cellstart[c.tot], wall_end = cellstart[2 * c.tot];
     const size_t n = (size_t)c.n;
     const bool short_list = nlist_s != nullptr;
@@ -233,85 +246,82 @@ k_neighbor_list(SimConst c, const double4* __restrict__ pos, const float4* __res
             // main.cpp:1416: a wall with no fluid neighbour gets no wall entries
             const bool take = active && !(kind == 1 && is_wall && cnt == 0);
             const int off = kind ? c.tot : 0;
-            for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-                for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-                    for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
-                        float gx, gy, gz;
-                        const int cx = slot(0, jx % w[0], gx), cy = slot(1, jy % w[1], gy),
-                                  cz = slot(2, jz % w[2], gz);
-                        const int cell = cell_id(c, cx, cy, cz);
-                        const float ox = (ALL3 || pf.use[0]) ? gx - fi.x : 0.f;
-                        const float oy = (ALL3 || pf.use[1]) ? gy - fi.y : 0.f;
-                        const float oz = (ALL3 || pf.use[2]) ? gz - fi.z : 0.f;
-                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
-                        for (int cb = b; cb < e; cb += 32) {
-                            // the candidates near the box, compacted in order into the stage
-                            bool near = false;
-                            float4 q;
-                            if (cb + lane < e) {
-                                q = pos32[cb + lane];
-                                const float ax = q.x + gx, ay = q.y + gy, az = q.z + gz;
-                                const float ex = (ALL3 || pf.use[0]) ? fmaxf(0.f, fmaxf(b0x - ax, ax - b1x)) : 0.f;
-                                const float ey = (ALL3 || pf.use[1]) ? fmaxf(0.f, fmaxf(b0y - ay, ay - b1y)) : 0.f;
-                                const float ez = (ALL3 || pf.use[2]) ? fmaxf(0.f, fmaxf(b0z - az, az - b1z)) : 0.f;
-                                near = __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, __fmul_rn(ez, ez))) <= pf.r2_box;
-                            }
-                            const unsigned kept = __ballot_sync(0xffffffffu, near);
-                            __syncwarp();
-                            if (near) {
-                                q.w = __int_as_float(lane);
-                                cw[__popc(kept & ((1u << lane) - 1u))] = q;
-                            }
-                            __syncwarp();
-                            const int m = __popc(kept);
-                            // per candidate of the stage: may be within rm (mask), needs the
-                            // FP64 test (exact: in a shell of the rm or the rs bound), within
-                            // rs for certain (in_s)
-                            unsigned mask = 0u, exact = 0u, in_s = 0u;
-                            if (take) {
-                                for (int t = 0; t < m; ++t) {
-                                    const float4 q = cw[t];
-                                    const float fx = (ALL3 || pf.use[0]) ? q.x + ox : 0.f;
-                                    const float fy = (ALL3 || pf.use[1]) ? q.y + oy : 0.f;
-                                    const float fz = (ALL3 || pf.use[2]) ? q.z + oz : 0.f;
-                                    // FMA: fewer roundings than the bound allows for
-                                    const float r2f = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, __fmul_rn(fz, fz)));
-                                    if (r2f <= pf.r2_hi) {
-                                        const unsigned bit = 1u << t;
-                                        mask |= bit;
-                                        if (r2f > pf.r2_lo || (short_list && r2f > pf.rs2_lo && r2f <= pf.rs2_hi))
-                                            exact |= bit;
-                                        else if (r2f <= pf.rs2_lo)
-                                            in_s |= bit;
-                                    }
-                                }
-                            }
-                            while (mask) {
-                                const int t = __ffs(mask) - 1;
-                                const unsigned bit = mask & (0u - mask);
-                                mask &= mask - 1u;
-                                const int j = cb + __float_as_int(cw[t].w);
-                                bool in = true, in_short = (in_s & bit) != 0u;
-                                if (exact & bit) {
-                                    const double4 pj = pos[j];
-                                    const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
-                                    const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
-                                    const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
-                                    const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
-                                    in = r2 <= c.rm2;
-                                    in_short = r2 <= c.rs2;
-                                }
-                                if (in) {
-                                    if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
-                                    cnt++;
-                                    if (short_list && in_short) {
-                                        if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
-                                        cnt_s++;
-                                    }
-                                }
+            for (int sl = 0; sl < nsl; ++sl) {
+                const int4 st = sten[wib][sl];
+                const int cell = st.x;
+                const float gx = __int_as_float(st.y), gy = __int_as_float(st.z), gz = __int_as_float(st.w);
+                const float ox = (ALL3 || pf.use[0]) ? gx - fi.x : 0.f;
+                const float oy = (ALL3 || pf.use[1]) ? gy - fi.y : 0.f;
+                const float oz = (ALL3 || pf.use[2]) ? gz - fi.z : 0.f;
+                const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                for (int cb = b; cb < e; cb += 32) {
+                    // the candidates near the box, compacted in order into the stage
+                    bool near = false;
+                    float4 q;
+                    if (cb + lane < e) {
+                        q = pos32[cb + lane];
+                        const float ax = q.x + gx, ay = q.y + gy, az = q.z + gz;
+                        const float ex = (ALL3 || pf.use[0]) ? fmaxf(0.f, fmaxf(b0x - ax, ax - b1x)) : 0.f;
+                        const float ey = (ALL3 || pf.use[1]) ? fmaxf(0.f, fmaxf(b0y - ay, ay - b1y)) : 0.f;
+                        const float ez = (ALL3 || pf.use[2]) ? fmaxf(0.f, fmaxf(b0z - az, az - b1z)) : 0.f;
+                        near = __fmaf_rn(ex, ex, __fmaf_rn(ey, ey, __fmul_rn(ez, ez))) <= pf.r2_box;
+                    }
+                    const unsigned kept = __ballot_sync(0xffffffffu, near);
+                    __syncwarp();
+                    if (near) {
+                        q.w = __int_as_float(lane);
+                        cw[__popc(kept & ((1u << lane) - 1u))] = q;
+                    }
+                    __syncwarp();
+                    const int m = __popc(kept);
+                    // per candidate of the stage: may be within rm (mask), needs the
+                    // FP64 test (exact: in a shell of the rm or the rs bound), within
+                    // rs for certain (in_s)
+                    unsigned mask = 0u, exact = 0u, in_s = 0u;
+                    if (take) {
+                        for (int t = 0; t < m; ++t) {
+                            const float4 q = cw[t];
+                            const float fx = (ALL3 || pf.use[0]) ? q.x + ox : 0.f;
+                            const float fy = (ALL3 || pf.use[1]) ? q.y + oy : 0.f;
+                            const float fz = (ALL3 || pf.use[2]) ? q.z + oz : 0.f;
+                            // FMA: fewer roundings than the bound allows for
+                            const float r2f = __fmaf_rn(fx, fx, __fmaf_rn(fy, fy, __fmul_rn(fz, fz)));
+                            if (r2f <= pf.r2_hi) {
+                                const unsigned bit = 1u << t;
+                                mask |= bit;
+                                if (r2f > pf.r2_lo || (short_list && r2f > pf.rs2_lo && r2f <= pf.rs2_hi))
+                                    exact |= bit;
+                                else if (r2f <= pf.rs2_lo)
+                                    in_s |= bit;
                             }
                         }
                     }
+                    while (mask) {
+                        const int t = __ffs(mask) - 1;
+                        const unsigned bit = mask & (0u - mask);
+                        mask &= mask - 1u;
+                        const int j = cb + __float_as_int(cw[t].w);
+                        bool in = true, in_short = (in_s & bit) != 0u;
+                        if (exact & bit) {
+                            const double4 pj = pos[j];
+                            const double q0 = omod_fast(pj.x - pi.x + c.half_width[0], c.width[0]) - c.half_width[0];
+                            const double q1 = omod_fast(pj.y - pi.y + c.half_width[1], c.width[1]) - c.half_width[1];
+                            const double q2 = omod_fast(pj.z - pi.z + c.half_width[2], c.width[2]) - c.half_width[2];
+                            const double r2 = q0 * q0 + q1 * q1 + q2 * q2;
+                            in = r2 <= c.rm2;
+                            in_short = r2 <= c.rs2;
+                        }
+                        if (in) {
+                            if (cnt < cap) nlist[(size_t)cnt * n + i] = j;
+                            cnt++;
+                            if (short_list && in_short) {
+                                if (cnt_s < cap_s) nlist_s[(size_t)cnt_s * n + i] = j;
+                                cnt_s++;
+                            }
+                        }
+                    }
+                }
+            }
         }
         if (active) {
             ncount[i] = cnt;
