@@ -224,6 +224,7 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
            unsigned* __restrict__ list, int cap_l, int* __restrict__ cnt_short, int* __restrict__ cnt_all,
            StepScalars* __restrict__ scal) {
     __shared__ float4 cand[kMixListWarps][32];
+    __shared__ int2 sten[kMixListWarps][27];  // the stencil in visiting order: cell, offset code
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int key = blockIdx.x * kMixListWarps + wib;
     if (key >= 2 * c.tot) return;  // whole warp
@@ -238,6 +239,19 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
         const int b = (2 * r) - (ic[d] + r) % c.cc[d];
         jmin[d] = b > 0 ? b : 0;
     }
+    // lane s < w0*w1*w2 computes stencil slot s of the visiting order (x
+    // outer, z inner), once for all the key's chunks
+    const int nsl = w[0] * w[1] * w[2];  // at most 27: range <= 1 on every axis
+    if (lane < nsl) {
+        const int ax = (jmin[0] + lane / (w[1] * w[2])) % w[0], ay = (jmin[1] + (lane / w[2]) % w[1]) % w[1],
+                  az = (jmin[2] + lane % w[2]) % w[2];
+        const int cx = ((ic[0] - c.range[0] + ax) % c.cc[0] + c.cc[0]) % c.cc[0];
+        const int cy = ((ic[1] - c.range[1] + ay) % c.cc[1] + c.cc[1]) % c.cc[1];
+        const int cz = ((ic[2] - c.range[2] + az) % c.cc[2] + c.cc[2]) % c.cc[2];
+        sten[wib][lane] = make_int2(cx * c.cc[1] * c.cc[2] + cy * c.cc[2] + cz,
+                                    (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1));
+    }
+    __syncwarp();
     const int nf = cellstart[c.tot];
     const size_t n = (size_t)c.n;
     const int cap_s = m.cap_s;
@@ -278,55 +292,49 @@ k_mix_list(SimConst c, MixConst m, const float4* __restrict__ p32, const int* __
             ++cnt;
         };
         bool any_fluid = !is_wall;  // a wall needs a list only if a fluid particle is within reach
-        for (int jx = jmin[0]; jx < jmin[0] + w[0]; ++jx)
-            for (int jy = jmin[1]; jy < jmin[1] + w[1]; ++jy)
-                for (int jz = jmin[2]; jz < jmin[2] + w[2]; ++jz) {
-                    const int ax = jx % w[0], ay = jy % w[1], az = jz % w[2];
-                    const int cx = ((ic[0] - c.range[0] + ax) % c.cc[0] + c.cc[0]) % c.cc[0];
-                    const int cy = ((ic[1] - c.range[1] + ay) % c.cc[1] + c.cc[1]) % c.cc[1];
-                    const int cz = ((ic[2] - c.range[2] + az) % c.cc[2] + c.cc[2]) % c.cc[2];
-                    const int cell = cx * c.cc[1] * c.cc[2] + cy * c.cc[2] + cz;
-                    const int code = (ax - c.range[0] + 1) * 9 + (ay - c.range[1] + 1) * 3 + (az - c.range[2] + 1);
-                    const float ox = m.dhi[code][0] - pi.x, oy = m.dhi[code][1] - pi.y, oz = m.dhi[code][2] - pi.z;
-                    for (int kind = 0; kind < 2; ++kind) {
-                        const int off = kind ? c.tot : 0;
-                        const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
-                        for (int cb = b; cb < e; cb += 32) {
-                            bool near = false;
-                            float4 qc;
-                            if (cb + lane < e) {
-                                qc = p32[cb + lane];
-                                const float ax = qc.x + m.dhi[code][0], ay = qc.y + m.dhi[code][1],
-                                            az = qc.z + m.dhi[code][2];
-                                const float ex = fmaxf(0.f, fmaxf(b0x - ax, ax - b1x));
-                                const float ey = fmaxf(0.f, fmaxf(b0y - ay, ay - b1y));
-                                const float ez = fmaxf(0.f, fmaxf(b0z - az, az - b1z));
-                                near = ex * ex + ey * ey + ez * ez < m.list_r2;
-                            }
-                            const unsigned kept = __ballot_sync(0xffffffffu, near);
-                            __syncwarp();
-                            if (near) {
-                                qc.w = __int_as_float(cb + lane);
-                                cw[__popc(kept & ((1u << lane) - 1u))] = qc;
-                            }
-                            __syncwarp();
-                            if (!active) continue;
-                            const int mm = __popc(kept);
-                            for (int t = 0; t < mm; ++t) {
-                                const float4 q = cw[t];
-                                const int j = __float_as_int(q.w);
-                                const float dx = q.x + ox, dy = q.y + oy, dz = q.z + oz;
-                                const float r2 = dx * dx + dy * dy + dz * dz;
-                                if (r2 < m.list_r2 && j != i) {
-                                    if (kind == 0) any_fluid = true;
-                                    const unsigned entry = ((unsigned)j << kCodeBits) | (unsigned)code;
-                                    if (r2 < m.short_r2) push(entry, cs, cap_s, ls, s0, s1, s2, s3);
-                                    else push(entry, cl, cap_l, ll, l0, l1, l2, l3);
-                                }
-                            }
+        for (int sl = 0; sl < nsl; ++sl) {
+            const int2 st = sten[wib][sl];
+            const int cell = st.x, code = st.y;
+            const float ox = m.dhi[code][0] - pi.x, oy = m.dhi[code][1] - pi.y, oz = m.dhi[code][2] - pi.z;
+            for (int kind = 0; kind < 2; ++kind) {
+                const int off = kind ? c.tot : 0;
+                const int b = cellstart[cell + off], e = cellstart[cell + off + 1];
+                for (int cb = b; cb < e; cb += 32) {
+                    bool near = false;
+                    float4 qc;
+                    if (cb + lane < e) {
+                        qc = p32[cb + lane];
+                        const float ax = qc.x + m.dhi[code][0], ay = qc.y + m.dhi[code][1],
+                                    az = qc.z + m.dhi[code][2];
+                        const float ex = fmaxf(0.f, fmaxf(b0x - ax, ax - b1x));
+                        const float ey = fmaxf(0.f, fmaxf(b0y - ay, ay - b1y));
+                        const float ez = fmaxf(0.f, fmaxf(b0z - az, az - b1z));
+                        near = ex * ex + ey * ey + ez * ez < m.list_r2;
+                    }
+                    const unsigned kept = __ballot_sync(0xffffffffu, near);
+                    __syncwarp();
+                    if (near) {
+                        qc.w = __int_as_float(cb + lane);
+                        cw[__popc(kept & ((1u << lane) - 1u))] = qc;
+                    }
+                    __syncwarp();
+                    if (!active) continue;
+                    const int mm = __popc(kept);
+                    for (int t = 0; t < mm; ++t) {
+                        const float4 q = cw[t];
+                        const int j = __float_as_int(q.w);
+                        const float dx = q.x + ox, dy = q.y + oy, dz = q.z + oz;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 < m.list_r2 && j != i) {
+                            if (kind == 0) any_fluid = true;
+                            const unsigned entry = ((unsigned)j << kCodeBits) | (unsigned)code;
+                            if (r2 < m.short_r2) push(entry, cs, cap_s, ls, s0, s1, s2, s3);
+                            else push(entry, cl, cap_l, ll, l0, l1, l2, l3);
                         }
                     }
                 }
+            }
+        }
         if (!active) continue;
         if ((cs & 3) != 0 && cs < cap_s) ls[(size_t)(cs >> 2) * n] = make_uint4(s0, s1, s2, s3);
         if ((cl & 3) != 0 && cl < cap_l) ll[(size_t)(cl >> 2) * n] = make_uint4(l0, l1, l2, l3);
